@@ -1,0 +1,420 @@
+"""Benchmark: split-precision tensor-core FP32 GEMM vs the FP32 SIMT kernel.
+
+One step = one C = A*B of the workload through the library (split pre-pass +
+tcgen05 GEMM for the headline), inputs resident in HBM. Default workload: the
+square 4096^3 FP32 GEMM of the square sweep (uniform [-1, 1) inputs, fixed
+seed), the shape the speed target is stated on.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--size S] [--precision tf32x3|bf16x6|bf16x9]
+
+Multi-GPU (torchrun, one rank per GPU): every rank multiplies its own M-row
+shard (a 4096 x 4096 block of A and the whole B); no collective touches the
+data path. Timing is on the device (CUDA events), max over ranks.
+
+The reference arm (--impl reference) times the reference's own CPU GEMM,
+Utils::multiply_scalar (common/utils.hpp:50-61) compiled into oracle/_ref, on
+the host's cores over a bounded sample of rows of the same product.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GFLOP/s & %roofline: split-precision TC vs FP32 SIMT GEMM at stated FP64 error"
+PREC = {"tf32x3": 1, "bf16x6": 2, "bf16x9": 3}
+PRODUCTS = {1: 3, 2: 6, 3: 9}
+
+
+def env_int(name: str, default: int) -> int:
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def measured_peaks() -> tuple[dict, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "sm_max_mhz": 1965.0}, \
+        "fallback"
+
+
+def traffic_from_profiles(name: str) -> float | None:
+    """DRAM bytes per launch of the dominant kernel, from a committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        for line in f:
+            if line.startswith("dram_bytes_per_launch:"):
+                try:
+                    return float(line.split(":", 1)[1].split()[0])
+                except ValueError:
+                    return None
+    return None
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.marks: list[tuple[float, float]] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu=timestamp,{self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", self.gpu_id], stdout=self.out, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            with open(self.out.name) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) < 10:
+                        continue
+                    try:
+                        rows.append({"sm": float(parts[2]), "max": float(parts[3]), "power": float(parts[4]),
+                                     "active": parts[5], "hw": parts[6], "hwt": parts[7], "swt": parts[8],
+                                     "pcap": parts[9]})
+                    except ValueError:
+                        continue
+        finally:
+            os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        loaded = [r for r in rows if r["power"] > 300.0] or rows
+        reasons = set()
+        for r in loaded:
+            if r["hw"].lower() == "active":
+                reasons.add("hw_slowdown")
+            if r["hwt"].lower() == "active":
+                reasons.add("hw_thermal_slowdown")
+            if r["swt"].lower() == "active":
+                reasons.add("sw_thermal_slowdown")
+            if r["pcap"].lower() == "active":
+                reasons.add("sw_power_cap")
+        return {"sm_mhz": statistics.median(r["sm"] for r in loaded), "sm_max_mhz": max(r["max"] for r in rows),
+                "reasons": sorted(reasons), "samples": len(loaded),
+                "power_w_max": max(r["power"] for r in loaded)}
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+def cpu_rows_gflops(A, B, K: int, N: int, budget_s: float, threads: int, start_row: int = 0) -> dict:
+    """The reference's multiply_scalar (oracle/_ref, else the oracle's
+    restatement) on whole rows of the product, `threads` host threads, for
+    about budget_s seconds. Returns GFLOP/s and what was sampled."""
+    import numpy as np
+    import oracle
+    if oracle.ref_available():
+        fn = oracle.ref().ref_multiply_scalar
+        kind = "reference"
+    else:
+        fn = oracle.lib().oracle_sgemm_scalar
+        kind = "port"
+    fp = ctypes.POINTER(ctypes.c_float)
+    Bp = B.ctypes.data_as(fp)
+    M = A.shape[0]
+    done_rows = [0] * threads
+    stop = time.perf_counter() + budget_s
+    out = np.empty((threads, N), np.float32)
+
+    def worker(t: int):
+        r = start_row + t
+        while time.perf_counter() < stop:
+            row = r % M
+            fn(A[row].ctypes.data_as(fp), Bp, out[t].ctypes.data_as(fp), 1, N, K)
+            done_rows[t] += 1
+            r += threads
+
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=worker, args=(t,)) for t in range(threads)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    dt = time.perf_counter() - t0
+    rows = sum(done_rows)
+    return {"value": 2.0 * rows * K * N / dt / 1e9, "unit": "GFLOP/s", "cores": threads, "kind": kind,
+            "sample": f"{rows} rows of the {M}x{K}x{N} product (1 x {K} x {N} each) in {dt:.1f} s",
+            "seconds": dt}
+
+
+def run_reference(args) -> None:
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    if rank != 0:
+        return
+    import numpy as np
+    import oracle
+    from maxmulsk_b200 import datagen
+    S = args.size
+    A = datagen.uniform(S * S, 11).reshape(S, S)
+    B = datagen.uniform(S * S, 12).reshape(S, S)
+    threads = os.cpu_count() or 1
+    oracle.lib()
+    # Each step: a bounded sample of rows, one row per host thread per step
+    # at least, sized so the whole run stays within a few minutes.
+    budget = max(0.05, min(2.0, 150.0 / max(1, args.steps + args.warmup)))
+    for w in range(args.warmup):
+        cpu_rows_gflops(A, B, S, S, budget, threads, start_row=w * threads)
+    vals, rows_total, secs = [], 0, 0.0
+    for s in range(args.steps):
+        r = cpu_rows_gflops(A, B, S, S, budget, threads, start_row=(args.warmup + s) * threads)
+        vals.append(r["value"])
+        secs += r["seconds"]
+        rows_total += int(r["sample"].split()[0])
+    value = 2.0 * rows_total * S * S / secs / 1e9
+    kind = "reference" if oracle.ref_available() else "port"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / max(1, args.steps),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded uniform [-1, 1))",
+        "config": {"workload": f"square {S}^3 FP32 GEMM, reference CPU path (Utils::multiply_scalar) on "
+                               f"row samples", "M": S, "K": S, "N": S},
+        "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": threads, "kind": kind,
+                         "sample": f"{rows_total} rows of the {S}^3 product over {args.steps} steps, "
+                                   f"{threads} threads"},
+        "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- ours
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=4096)
+    ap.add_argument("--precision", choices=list(PREC), default="tf32x3")
+    ap.add_argument("--no-extras", action="store_true", help="headline timing only (for profiling runs)")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import maxmulsk_b200 as mm
+    from maxmulsk_b200 import datagen
+
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    S = args.size
+    M = K = N = S
+    prec = PREC[args.precision]
+    # This rank's M-row shard of an (world*S) x S x S product: its own rows of A.
+    A = datagen.uniform(M * K, 11 + 1000 * rank).reshape(M, K)
+    B = datagen.uniform(K * N, 12).reshape(K, N)
+    dA = torch.from_numpy(A).to(dev)
+    dB = torch.from_numpy(B).to(dev)
+    dC = torch.empty((M, N), dtype=torch.float32, device=dev)
+    dCs = torch.empty((M, N), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    plan = mm.choose(M, K, N, prec)
+    ws_bytes = mm.workspace_bytes(M, K, N, plan)
+    ws = torch.empty(ws_bytes + 256, dtype=torch.uint8, device=dev)
+    wsp = ws.data_ptr() + ((-ws.data_ptr()) % 256)
+    reuse = mm.make_plan(plan.precision, plan.tile_m, plan.tile_n, plan.split_k, mm.TC_REUSE_PLANES)
+
+    def step_tc():
+        mm.check(mm.sgemm_plan_dev(dA, dB, dC, M, K, N, plan, wsp, ws_bytes, stream), "tc step")
+
+    def step_gemm_only():
+        mm.check(mm.sgemm_plan_dev(dA, dB, dC, M, K, N, reuse, wsp, ws_bytes, stream), "tc gemm")
+
+    splan = mm.choose(M, K, N, mm.Precision.FP32)
+    sws_bytes = mm.workspace_bytes(M, K, N, splan)
+    sws = torch.empty(sws_bytes + 256, dtype=torch.uint8, device=dev)
+    swsp = sws.data_ptr() + ((-sws.data_ptr()) % 256)
+
+    def step_simt():
+        mm.check(mm.sgemm_plan_dev(dA, dB, dCs, M, K, N, splan, swsp, sws_bytes, stream), "simt step")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn, steps: int) -> float:
+        """Seconds per step: CUDA events on the launching stream, synchronize on both sides."""
+        barrier()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / 1e3 / steps)
+
+    gpu_uuid = str(local)
+    try:
+        gpu_uuid = str(torch.cuda.get_device_properties(dev).uuid)
+        if not gpu_uuid.startswith("GPU-"):
+            gpu_uuid = "GPU-" + gpu_uuid
+    except Exception:
+        pass
+
+    # ---- headline: split pre-pass + tcgen05 GEMM, K timed steps
+    for _ in range(args.warmup):
+        step_tc()
+    mm.check(mm.stream_status(stream), "warm-up status")
+    sampler = ClockSampler(gpu_uuid)
+    sampler.start()
+    time.sleep(0.3)
+    t_step = timed(step_tc, args.steps)
+    sampler.stop()
+    mm.check(mm.stream_status(stream), "timed status")
+    clocks = sampler.summary()
+    flops = 2.0 * M * N * K
+    value = flops * world / t_step / 1e9
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform [-1, 1), SplitMix64)",
+        "config": {"workload": f"square {S}^3 FP32 GEMM, {args.precision} split tensor-core kernel "
+                               f"(split pre-pass + tcgen05 GEMM); per-rank M-row shard",
+                   "M": M, "K": K, "N": N, "precision": args.precision,
+                   "plan": {"tile_m": plan.tile_m, "tile_n": plan.tile_n, "split_k": plan.split_k},
+                   "l2": f"inputs larger than L2: A+B+C = {3 * S * S * 4 / 2**20:.0f} MiB, planes "
+                         f"{ws_bytes / 2**20:.0f} MiB > 126 MB", "parallelism": f"replicas x{world} (M-row shards)"},
+        "clocks": clocks,
+        "gpu_launches": 3 * args.steps,
+    }
+
+    if not args.no_extras:
+        peaks, peak_src = measured_peaks()
+        # ---- the GEMM kernel alone (planes already split), for the roofline
+        n_k = max(20, min(args.steps, 200))
+        for _ in range(3):
+            step_gemm_only()
+        t_gemm = timed(step_gemm_only, n_k)
+        tf32_peak = peaks["bf16_tflops"] / 2.0         # TF32 dense = half the BF16 rate
+        mode_peak = (tf32_peak if prec == 1 else peaks["bf16_tflops"]) / PRODUCTS[prec]
+        achieved = flops / t_gemm / 1e12
+        traffic = traffic_from_profiles(f"tc_gemm_{args.precision}_{S}.txt")
+        out["roofline"] = {
+            "bound": "tensor", "achieved": achieved, "peak": mode_peak, "unit": "TFLOP/s",
+            "frac": achieved / mode_peak, "traffic": traffic,
+            "kernel": "tc_gemm_kernel (GEMM alone, planes already split)",
+            "peak_basis": f"{peak_src} bf16 burst {peaks['bf16_tflops']} TF/s"
+                          f"{' / 2 (TF32 rate)' if prec == 1 else ''} / {PRODUCTS[prec]} products; useful 2MNK flops",
+            "gemm_ms": t_gemm * 1e3, "prepass_ms": max(0.0, (t_step - t_gemm) * 1e3),
+        }
+        # ---- the FP32 SIMT kernel on the same inputs
+        for _ in range(3):
+            step_simt()
+        t_simt = timed(step_simt, max(10, min(args.steps, 100)))
+        simt_gf = flops / t_simt / 1e9
+        sm_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+        fp32_peak_max = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+        out["simt"] = {"gflops": simt_gf, "ms_per_step": t_simt * 1e3,
+                       "plan": {"tile_m": splan.tile_m, "tile_n": splan.tile_n, "split_k": splan.split_k},
+                       "peak_tflops": fp32_peak_max, "frac": simt_gf / 1e3 / fp32_peak_max,
+                       "peak_basis": "nominal FP32 FMA: 148 SMs x 128 lanes x 2 x max SM clock"}
+        out["speedup_vs_simt"] = (flops / t_step) / (flops / t_simt)
+        out["speedup_vs_simt_gemm_only"] = t_simt / t_gemm
+        out["gpu_launches"] = 3 * args.steps
+        # ---- FP64-measured error of both kernels (cuBLAS DGEMM as the FP64 product, outside timing)
+        if rank == 0:
+            with torch.no_grad():
+                A64, B64 = dA.double(), dB.double()
+                C64 = A64 @ B64
+                floor = (A64.abs() @ B64.abs()) * 2.0 ** -24
+                nab = torch.linalg.norm(A64) * torch.linalg.norm(B64)
+                errs = {}
+                for name, Cx in (("tc", dC), ("simt", dCs)):
+                    d = (Cx.double() - C64).abs()
+                    errs[name] = {"normwise": float(torch.linalg.norm(d) / nab),
+                                  "max_rel": float((d / torch.maximum(C64.abs(), floor)).max())}
+                del A64, B64, C64, floor
+            errs["tc_over_simt_normwise"] = errs["tc"]["normwise"] / errs["simt"]["normwise"]
+            out["fp64_error"] = errs
+        # ---- end to end through the public host-pointer API (pinned host buffers)
+        hA = torch.from_numpy(A).pin_memory()
+        hB = torch.from_numpy(B).pin_memory()
+        hC = torch.empty((M, N), dtype=torch.float32).pin_memory()
+        e2e_steps = max(3, min(args.steps, 30))
+        lib = mm.lib()
+        for _ in range(2):
+            mm.check(lib.maxmulsk_sgemm_split(hA.data_ptr(), hB.data_ptr(), hC.data_ptr(), M, K, N, prec), "e2e")
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            mm.check(lib.maxmulsk_sgemm_split(hA.data_ptr(), hB.data_ptr(), hC.data_ptr(), M, K, N, prec), "e2e")
+        t_e2e = max_over_ranks((time.perf_counter() - t0) / e2e_steps)
+        out["e2e"] = {"value": flops * world / t_e2e / 1e9, "unit": "GFLOP/s",
+                      "h2d_bytes_per_step": 4 * (M * K + K * N), "d2h_bytes_per_step": 4 * M * N,
+                      "ms_per_step": t_e2e * 1e3, "steps": e2e_steps,
+                      "api": "maxmulsk_sgemm_split (host pointers, synchronous, pinned buffers)"}
+        # ---- the reference's CPU path, rank 0 at N = 1 only
+        if world == 1 and rank == 0:
+            out["cpu_baseline"] = cpu_rows_gflops(A, B, K, N, budget_s=12.0, threads=1)
+            out["cpu_baseline"].pop("seconds", None)
+
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

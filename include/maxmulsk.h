@@ -1,0 +1,188 @@
+#pragma once
+/*
+ * MaxMulSK-B200: row-major FP32 GEMM C = A*B on NVIDIA B200 (sm_100a).
+ *
+ * Drop-in for the reference's C ABI (capi/maxmulsk.h:9-41). Every function
+ * computes C = A*B for row-major, tightly packed FP32 matrices: A is M x K,
+ * B is K x N, C is M x N. C is overwritten (alpha = 1, beta = 0); its previous
+ * contents are never read. Dimensions follow the reference's (M, K, N) order,
+ * not BLAS's (M, N, K).
+ *
+ * Empty shapes follow the reference (capi/maxmulsk.cpp:13-20): M == 0 or
+ * N == 0 returns MAXMULSK_OK without touching anything; K == 0 sets C to zero.
+ *
+ * The header names no CUDA type. A stream is passed as `void*` holding a
+ * cudaStream_t (NULL = the legacy default stream). Device pointers are plain
+ * pointers to memory of the current CUDA device.
+ *
+ * Thread safety: calls from several host threads are safe. Workspace is kept
+ * per (device, stream); the tuning database is loaded once under a mutex.
+ */
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The first three keep the reference's values
+ * (capi/maxmulsk.h:24-28); the rest are appended, never renumbered. */
+typedef enum {
+    MAXMULSK_OK = 0,
+    MAXMULSK_ERR_UNSUPPORTED,   /* the plan or shape was rejected; C untouched   */
+    MAXMULSK_ERR_ALLOC,         /* a device or pinned buffer could not be had     */
+    MAXMULSK_ERR_CUDA,          /* a CUDA runtime/driver call failed              */
+    MAXMULSK_ERR_INVALID,       /* a null pointer, or a workspace that is too small */
+    MAXMULSK_ERR_TIMEOUT,       /* a bounded device-side wait gave up             */
+} maxmulsk_status;
+
+/* ----------------------------------------------------------------------------
+ * Drop-in entry points (host pointers, synchronous, FP32-SIMT accurate).
+ * Each copies A and B to the current device, multiplies, copies C back and
+ * waits. Pinned (page-locked) host buffers are copied directly; pageable ones
+ * go through a pinned staging ring.
+ * ------------------------------------------------------------------------- */
+
+/* Replaces capi/maxmulsk.h:32-33 (SMEKernels1x4AccKcOut). The plan comes from
+ * the tuning picker (tuning database, else the learned cost model, else the
+ * shape rule), FP32 SIMT precision; MAXMULSK_CONFIG overrides it. Unlike the
+ * reference's v3, allocation failure is reported (MAXMULSK_ERR_ALLOC). */
+maxmulsk_status maxmulsk_sgemm_v3(const float* A, const float* B, float* C,
+                                  size_t M, size_t K, size_t N);
+
+/* Replaces capi/maxmulsk.h:36-37 (the v4c dispatcher): a fixed shape rule
+ * picks between two plans, as sme/v4/sme-1x4-v4c-dispatch.cpp:17-22 does;
+ * no database and no environment override. FP32 SIMT precision. */
+maxmulsk_status maxmulsk_sgemm_v4(const float* A, const float* B, float* C,
+                                  size_t M, size_t K, size_t N);
+
+/* ----------------------------------------------------------------------------
+ * Device-pointer variants: asynchronous on `stream`. Errors detected on the
+ * host are returned at once; a device-side timeout is reported by
+ * maxmulsk_stream_status().
+ * ------------------------------------------------------------------------- */
+maxmulsk_status maxmulsk_sgemm_v3_dev(const float* dA, const float* dB, float* dC,
+                                      size_t M, size_t K, size_t N, void* stream);
+maxmulsk_status maxmulsk_sgemm_v4_dev(const float* dA, const float* dB, float* dC,
+                                      size_t M, size_t K, size_t N, void* stream);
+
+/* ----------------------------------------------------------------------------
+ * Precision and plans.
+ * ------------------------------------------------------------------------- */
+typedef enum {
+    MAXMULSK_PREC_FP32   = 0,   /* FP32 FMA on the CUDA cores                    */
+    MAXMULSK_PREC_3XTF32 = 1,   /* tensor cores: hi*hi + hi*lo + lo*hi, TF32      */
+    MAXMULSK_PREC_BF16X6 = 2,   /* tensor cores: 3 BF16 limbs, pairs i+j <= 2     */
+    MAXMULSK_PREC_BF16X9 = 3,   /* tensor cores: 3 BF16 limbs, all nine pairs     */
+} maxmulsk_precision;
+
+/* Kernel variants inside MAXMULSK_PREC_FP32. */
+enum {
+    MAXMULSK_FP32_FMA    = 0,   /* one fused multiply-add per k step             */
+    MAXMULSK_FP32_SCALAR = 1,   /* multiply then add per k step, the arithmetic of
+                                   Utils::multiply_scalar (common/utils.hpp:50-61) */
+};
+
+/* Variants of the tensor-core precisions. */
+enum {
+    MAXMULSK_TC_SPLIT_INPUTS = 0,  /* split A and B into operand planes, then multiply */
+    MAXMULSK_TC_REUSE_PLANES = 1,  /* the workspace already holds the planes of these
+                                      A and B (a previous call with the same inputs,
+                                      shape, precision and workspace): skip the split */
+};
+
+/* The analog of the reference's Blocking (sme/v4/sme-1x4-kcout-ncblock-apack4za.hpp:30,
+ * sme/support/gemm_tuning.hpp:37-43): how one GEMM is cut into work.
+ *   precision : maxmulsk_precision
+ *   tile_m, tile_n : output tile of one CTA. FP32: 128x128, 128x64, 64x64.
+ *                    Tensor cores: tile_m 128, tile_n 64, 128 or 256.
+ *   split_k   : number of K slices (1..64). Slices are summed in slice order,
+ *               first slice first, like the reference's outer-Kc panels
+ *               (sme/v3/sme-1x4-acc-kcout.cpp:464-471, 530-558).
+ *   variant   : FP32: MAXMULSK_FP32_FMA or MAXMULSK_FP32_SCALAR.
+ *               Tensor cores: MAXMULSK_TC_SPLIT_INPUTS or MAXMULSK_TC_REUSE_PLANES. */
+typedef struct {
+    int32_t precision;
+    int32_t tile_m;
+    int32_t tile_n;
+    int32_t split_k;
+    int32_t variant;
+    int32_t reserved[3];
+} maxmulsk_plan;
+
+/* Validates a plan for a shape (the analog of NB::classify,
+ * sme/v4/sme-1x4-kcout-ncblock-apack4za.cpp:410-423): MAXMULSK_OK or
+ * MAXMULSK_ERR_UNSUPPORTED. A rejected plan never touches C. */
+maxmulsk_status maxmulsk_classify(size_t M, size_t K, size_t N, const maxmulsk_plan* plan);
+
+/* The picker behind maxmulsk_sgemm_v3 for a given precision (the analog of
+ * MaxMulSK::tuning::select, sme/support/gemm_tuning.cpp:96-100). */
+maxmulsk_status maxmulsk_choose(size_t M, size_t K, size_t N, int32_t precision,
+                                maxmulsk_plan* out);
+
+/* The fixed shape rule behind maxmulsk_sgemm_v4 (the analog of
+ * SMEKernels1x4V4C::choose, sme/v4/sme-1x4-v4c-dispatch.cpp:17-22). */
+maxmulsk_status maxmulsk_choose_rule(size_t M, size_t K, size_t N, int32_t precision,
+                                     maxmulsk_plan* out);
+
+/* Device workspace a plan needs (the analog of workspace_bytes,
+ * sme/v5/sme-1x4-fusedpack-v51.hpp:75-78, and NB::capacity,
+ * sme/v4/sme-1x4-kcout-ncblock-apack4za.cpp:429-444). 0 when none. */
+size_t maxmulsk_workspace_bytes(size_t M, size_t K, size_t N, const maxmulsk_plan* plan);
+
+/* Explicit plan, caller-owned device workspace (no allocation inside the
+ * call; the analog of run_multiplication_ws, sme/v5/sme-1x4-fusedpack-v51.hpp:76-78).
+ * ws must be 256-byte aligned and at least maxmulsk_workspace_bytes() long;
+ * ws may be NULL when that is 0. Asynchronous on `stream`. */
+maxmulsk_status maxmulsk_sgemm_plan_dev(const float* dA, const float* dB, float* dC,
+                                        size_t M, size_t K, size_t N,
+                                        const maxmulsk_plan* plan,
+                                        void* ws, size_t ws_bytes, void* stream);
+
+/* Explicit plan on host pointers, synchronous (workspace managed inside). */
+maxmulsk_status maxmulsk_sgemm_plan(const float* A, const float* B, float* C,
+                                    size_t M, size_t K, size_t N,
+                                    const maxmulsk_plan* plan);
+
+/* Split-precision tensor-core GEMM, selected explicitly (the plain names stay
+ * FP32 SIMT). precision is one of MAXMULSK_PREC_3XTF32 / _BF16X6 / _BF16X9. */
+maxmulsk_status maxmulsk_sgemm_split(const float* A, const float* B, float* C,
+                                     size_t M, size_t K, size_t N, int32_t precision);
+maxmulsk_status maxmulsk_sgemm_split_dev(const float* dA, const float* dB, float* dC,
+                                         size_t M, size_t K, size_t N, int32_t precision,
+                                         void* stream);
+
+/* TEST ONLY: writes the operand planes the split pre-pass makes from one
+ * row-major R x C FP32 matrix, exactly as the tensor-core path does (the
+ * analog of NB::probe_pack_A / probe_pack_B,
+ * sme/v4/sme-1x4-kcout-ncblock-apack4za.hpp:44-49). as_b == 0 lays planes
+ * out as A ([P][R][Cp], Cp = C padded to 16 bytes); as_b != 0 as B
+ * ([P][Cp/NBE][R][NBE], Cp = C padded to 128 bytes, NBE = 128 bytes of
+ * elements). Planes are FP32 (3xTF32, P = 2) or BF16 (P = 3), each plane
+ * starting at a multiple of 1 KiB; out must hold
+ * maxmulsk_probe_split_bytes() bytes. Asynchronous on `stream`. */
+size_t maxmulsk_probe_split_bytes(size_t R, size_t C, int32_t precision, int32_t as_b);
+maxmulsk_status maxmulsk_probe_split_dev(const float* dX, size_t R, size_t C, int32_t precision,
+                                         int32_t as_b, void* out, void* stream);
+
+/* ----------------------------------------------------------------------------
+ * Status, errors, device properties.
+ * ------------------------------------------------------------------------- */
+
+/* Waits for `stream` and returns MAXMULSK_ERR_TIMEOUT if any kernel of this
+ * library on the current device gave up a bounded wait since the last call
+ * (the flag is then cleared), MAXMULSK_ERR_CUDA on a CUDA error, else OK. */
+maxmulsk_status maxmulsk_stream_status(void* stream);
+
+/* A static, human-readable name for a status. */
+const char* maxmulsk_status_string(maxmulsk_status s);
+
+/* The text of the last CUDA error this thread saw inside the library. */
+const char* maxmulsk_last_error_message(void);
+
+/* Library version, e.g. "0.1.0". */
+const char* maxmulsk_version(void);
+
+#ifdef __cplusplus
+}
+#endif

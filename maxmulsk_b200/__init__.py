@@ -1,0 +1,254 @@
+"""MaxMulSK-B200: row-major FP32 GEMM C = A*B on NVIDIA B200 (sm_100a).
+
+Python mirror of the C ABI in include/maxmulsk.h (itself the drop-in for the
+reference's capi/maxmulsk.h). Same names, same (M, K, N) argument order, same
+status codes; C is overwritten and never read.
+
+Host entry points take numpy float32 arrays (C-contiguous); device entry
+points take torch CUDA tensors or raw device pointers (int). Every call goes
+through libmaxmulsk_b200.so; nothing here computes a product on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+from typing import Any
+
+from . import _lib
+from ._lib import Plan, Problem
+
+__version__ = "0.1.0"
+
+
+class Status(enum.IntEnum):
+    OK = 0
+    ERR_UNSUPPORTED = 1
+    ERR_ALLOC = 2
+    ERR_CUDA = 3
+    ERR_INVALID = 4
+    ERR_TIMEOUT = 5
+
+
+class Precision(enum.IntEnum):
+    FP32 = 0
+    TF32X3 = 1
+    BF16X6 = 2
+    BF16X9 = 3
+
+
+FP32_FMA = 0
+FP32_SCALAR = 1
+TC_SPLIT_INPUTS = 0
+TC_REUSE_PLANES = 1
+
+
+class MaxMulSKError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = Status(status) if status in Status._value2member_map_ else status
+        msg = lib().maxmulsk_last_error_message()
+        super().__init__(f"{where}: {self.status!s} ({(msg or b'').decode(errors='replace')})")
+
+
+def lib() -> ctypes.CDLL:
+    return _lib.load()
+
+
+def _host_ptr(x: Any, n: int, name: str, writable: bool = False) -> int | None:
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    import numpy as np
+    if not isinstance(x, np.ndarray):
+        raise TypeError(f"{name} must be a numpy array or an int pointer")
+    if x.dtype != np.float32 or not x.flags.c_contiguous:
+        raise TypeError(f"{name} must be a C-contiguous float32 array")
+    if x.size < n:
+        raise ValueError(f"{name} has {x.size} elements, needs {n}")
+    if writable and not x.flags.writeable:
+        raise ValueError(f"{name} is read-only")
+    return x.ctypes.data
+
+
+def _dev_ptr(x: Any, n: int, name: str) -> int | None:
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    try:
+        import torch
+    except ImportError as e:  # pragma: no cover
+        raise TypeError(f"{name}: device entry points take torch tensors or int pointers") from e
+    if not isinstance(x, torch.Tensor) or not x.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor or an int pointer")
+    if x.dtype != torch.float32 or not x.is_contiguous():
+        raise TypeError(f"{name} must be a contiguous float32 CUDA tensor")
+    if x.numel() < n:
+        raise ValueError(f"{name} has {x.numel()} elements, needs {n}")
+    return x.data_ptr()
+
+
+def _stream_ptr(stream: Any) -> int | None:
+    if stream is None:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return torch.cuda.current_stream().cuda_stream
+        except ImportError:  # pragma: no cover
+            pass
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+# --------------------------------------------------------------------------- host
+def sgemm_v3(A, B, C, M: int, K: int, N: int) -> Status:
+    """C = A*B on host buffers; the tuned FP32 SIMT plan (capi/maxmulsk.h:32-33)."""
+    return Status(lib().maxmulsk_sgemm_v3(_host_ptr(A, M * K, "A"), _host_ptr(B, K * N, "B"),
+                                          _host_ptr(C, M * N, "C", True), M, K, N))
+
+
+def sgemm_v4(A, B, C, M: int, K: int, N: int) -> Status:
+    """C = A*B on host buffers; the fixed-rule FP32 SIMT plan (capi/maxmulsk.h:36-37)."""
+    return Status(lib().maxmulsk_sgemm_v4(_host_ptr(A, M * K, "A"), _host_ptr(B, K * N, "B"),
+                                          _host_ptr(C, M * N, "C", True), M, K, N))
+
+
+def sgemm_plan(A, B, C, M: int, K: int, N: int, plan: Plan) -> Status:
+    return Status(lib().maxmulsk_sgemm_plan(_host_ptr(A, M * K, "A"), _host_ptr(B, K * N, "B"),
+                                            _host_ptr(C, M * N, "C", True), M, K, N, ctypes.byref(plan)))
+
+
+def sgemm_split(A, B, C, M: int, K: int, N: int, precision: int = Precision.TF32X3) -> Status:
+    return Status(lib().maxmulsk_sgemm_split(_host_ptr(A, M * K, "A"), _host_ptr(B, K * N, "B"),
+                                             _host_ptr(C, M * N, "C", True), M, K, N, int(precision)))
+
+
+# --------------------------------------------------------------------------- device
+def sgemm_v3_dev(dA, dB, dC, M: int, K: int, N: int, stream=None) -> Status:
+    return Status(lib().maxmulsk_sgemm_v3_dev(_dev_ptr(dA, M * K, "A"), _dev_ptr(dB, K * N, "B"),
+                                              _dev_ptr(dC, M * N, "C"), M, K, N, _stream_ptr(stream)))
+
+
+def sgemm_v4_dev(dA, dB, dC, M: int, K: int, N: int, stream=None) -> Status:
+    return Status(lib().maxmulsk_sgemm_v4_dev(_dev_ptr(dA, M * K, "A"), _dev_ptr(dB, K * N, "B"),
+                                              _dev_ptr(dC, M * N, "C"), M, K, N, _stream_ptr(stream)))
+
+
+def sgemm_plan_dev(dA, dB, dC, M: int, K: int, N: int, plan: Plan, ws=None, ws_bytes: int = 0,
+                   stream=None) -> Status:
+    wsp = None
+    if ws is not None:
+        wsp = ws if isinstance(ws, int) else ws.data_ptr()
+        if not isinstance(ws, int) and not ws_bytes:
+            ws_bytes = ws.numel() * ws.element_size()
+    return Status(lib().maxmulsk_sgemm_plan_dev(_dev_ptr(dA, M * K, "A"), _dev_ptr(dB, K * N, "B"),
+                                                _dev_ptr(dC, M * N, "C"), M, K, N, ctypes.byref(plan),
+                                                wsp, ws_bytes, _stream_ptr(stream)))
+
+
+def sgemm_split_dev(dA, dB, dC, M: int, K: int, N: int, precision: int = Precision.TF32X3,
+                    stream=None) -> Status:
+    return Status(lib().maxmulsk_sgemm_split_dev(_dev_ptr(dA, M * K, "A"), _dev_ptr(dB, K * N, "B"),
+                                                 _dev_ptr(dC, M * N, "C"), M, K, N, int(precision),
+                                                 _stream_ptr(stream)))
+
+
+# --------------------------------------------------------------------------- plans
+def make_plan(precision: int = Precision.FP32, tile_m: int = 128, tile_n: int = 128, split_k: int = 1,
+              variant: int = 0) -> Plan:
+    p = Plan()
+    p.precision, p.tile_m, p.tile_n, p.split_k, p.variant = int(precision), tile_m, tile_n, split_k, variant
+    return p
+
+
+def classify(M: int, K: int, N: int, plan: Plan) -> Status:
+    return Status(lib().maxmulsk_classify(M, K, N, ctypes.byref(plan)))
+
+
+def choose(M: int, K: int, N: int, precision: int = Precision.FP32) -> Plan:
+    p = Plan()
+    st = lib().maxmulsk_choose(M, K, N, int(precision), ctypes.byref(p))
+    if st != 0:
+        raise MaxMulSKError(st, "maxmulsk_choose")
+    return p
+
+
+def choose_rule(M: int, K: int, N: int, precision: int = Precision.FP32) -> Plan:
+    p = Plan()
+    st = lib().maxmulsk_choose_rule(M, K, N, int(precision), ctypes.byref(p))
+    if st != 0:
+        raise MaxMulSKError(st, "maxmulsk_choose_rule")
+    return p
+
+
+def workspace_bytes(M: int, K: int, N: int, plan: Plan) -> int:
+    return int(lib().maxmulsk_workspace_bytes(M, K, N, ctypes.byref(plan)))
+
+
+def slice_len(K: int, split_k: int) -> int:
+    """K slice length of a plan (the kernels' rule, internal.hpp slice_len)."""
+    if split_k <= 1 or K == 0:
+        return K
+    per = (K + split_k - 1) // split_k
+    per = (per + 31) // 32 * 32
+    return min(per, K)
+
+
+def stream_status(stream=None) -> Status:
+    return Status(lib().maxmulsk_stream_status(_stream_ptr(stream)))
+
+
+def status_string(s: int) -> str:
+    return lib().maxmulsk_status_string(int(s)).decode()
+
+
+def last_error_message() -> str:
+    return (lib().maxmulsk_last_error_message() or b"").decode(errors="replace")
+
+
+def version() -> str:
+    return lib().maxmulsk_version().decode()
+
+
+def check(status: int, where: str = "maxmulsk") -> None:
+    if status != 0:
+        raise MaxMulSKError(status, where)
+
+
+def matmul(a, b, precision: int = Precision.FP32, plan: Plan | None = None, stream=None):
+    """torch convenience: returns a new CUDA tensor C = a @ b (float32, row-major)."""
+    import torch
+    M, K = a.shape
+    K2, N = b.shape
+    if K != K2:
+        raise ValueError("inner dimensions differ")
+    c = torch.empty((M, N), device=a.device, dtype=torch.float32)
+    if plan is not None:
+        st = sgemm_plan_dev(a, b, c, M, K, N, plan, stream=stream) if workspace_bytes(M, K, N, plan) == 0 \
+            else _plan_with_ws(a, b, c, M, K, N, plan, stream)
+    elif int(precision) == Precision.FP32:
+        st = sgemm_v3_dev(a, b, c, M, K, N, stream)
+    else:
+        st = sgemm_split_dev(a, b, c, M, K, N, precision, stream)
+    check(st, "matmul")
+    return c
+
+
+def _plan_with_ws(a, b, c, M, K, N, plan, stream):
+    import torch
+    nb = workspace_bytes(M, K, N, plan)
+    ws = torch.empty(nb + 256, dtype=torch.uint8, device=a.device)
+    off = (-ws.data_ptr()) % 256
+    return sgemm_plan_dev(a, b, c, M, K, N, plan, ws.data_ptr() + off, nb, stream)
+
+
+__all__ = [
+    "Status", "Precision", "Plan", "Problem", "FP32_FMA", "FP32_SCALAR", "TC_SPLIT_INPUTS", "TC_REUSE_PLANES",
+    "MaxMulSKError",
+    "sgemm_v3", "sgemm_v4", "sgemm_plan", "sgemm_split",
+    "sgemm_v3_dev", "sgemm_v4_dev", "sgemm_plan_dev", "sgemm_split_dev",
+    "make_plan", "classify", "choose", "choose_rule", "workspace_bytes", "slice_len",
+    "stream_status", "status_string", "last_error_message", "version", "check", "matmul", "lib",
+]

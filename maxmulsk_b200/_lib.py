@@ -1,0 +1,114 @@
+"""ctypes bindings for libmaxmulsk_b200.so (the C ABI in include/maxmulsk.h).
+
+The library is built in-tree by ``maxmulsk_b200.build``. Loading fails loudly
+when it is missing: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_float, c_int32, c_size_t, c_void_p
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libmaxmulsk_b200.so")
+
+
+class Plan(ctypes.Structure):
+    """maxmulsk_plan: how one GEMM is cut into work."""
+
+    _fields_ = [
+        ("precision", c_int32),
+        ("tile_m", c_int32),
+        ("tile_n", c_int32),
+        ("split_k", c_int32),
+        ("variant", c_int32),
+        ("reserved", c_int32 * 3),
+    ]
+
+    def __repr__(self) -> str:
+        return (f"Plan(precision={self.precision}, tile_m={self.tile_m}, tile_n={self.tile_n}, "
+                f"split_k={self.split_k}, variant={self.variant})")
+
+    def as_tuple(self) -> tuple[int, int, int, int, int]:
+        return (self.precision, self.tile_m, self.tile_n, self.split_k, self.variant)
+
+
+class Problem(ctypes.Structure):
+    """maxmulsk_problem: one GEMM of a grouped launch (device pointers)."""
+
+    _fields_ = [
+        ("A", c_void_p),
+        ("B", c_void_p),
+        ("C", c_void_p),
+        ("M", c_size_t),
+        ("K", c_size_t),
+        ("N", c_size_t),
+    ]
+
+
+# name -> (restype, argtypes)
+_SIGNATURES: dict[str, tuple] = {
+    "maxmulsk_sgemm_v3": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t]),
+    "maxmulsk_sgemm_v4": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t]),
+    "maxmulsk_sgemm_v3_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t, c_void_p]),
+    "maxmulsk_sgemm_v4_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t, c_void_p]),
+    "maxmulsk_classify": (c_int32, [c_size_t, c_size_t, c_size_t, POINTER(Plan)]),
+    "maxmulsk_choose": (c_int32, [c_size_t, c_size_t, c_size_t, c_int32, POINTER(Plan)]),
+    "maxmulsk_choose_rule": (c_int32, [c_size_t, c_size_t, c_size_t, c_int32, POINTER(Plan)]),
+    "maxmulsk_workspace_bytes": (c_size_t, [c_size_t, c_size_t, c_size_t, POINTER(Plan)]),
+    "maxmulsk_sgemm_plan_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t,
+                                          POINTER(Plan), c_void_p, c_size_t, c_void_p]),
+    "maxmulsk_sgemm_plan": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t,
+                                      POINTER(Plan)]),
+    "maxmulsk_sgemm_split": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t, c_int32]),
+    "maxmulsk_sgemm_split_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t,
+                                           c_int32, c_void_p]),
+    "maxmulsk_probe_split_bytes": (c_size_t, [c_size_t, c_size_t, c_int32, c_int32]),
+    "maxmulsk_probe_split_dev": (c_int32, [c_void_p, c_size_t, c_size_t, c_int32, c_int32, c_void_p, c_void_p]),
+    "maxmulsk_stream_status": (c_int32, [c_void_p]),
+    "maxmulsk_status_string": (c_char_p, [c_int32]),
+    "maxmulsk_last_error_message": (c_char_p, []),
+    "maxmulsk_version": (c_char_p, []),
+}
+
+_lib: ctypes.CDLL | None = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads the CUDA library once; raises ImportError if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m maxmulsk_b200.build` "
+            "(nvcc, sm_100a). There is no CPU fallback.")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    """Names every header in include/ declares (parsed from the header text)."""
+    import re
+    inc = os.path.join(os.path.dirname(HERE), "include")
+    names: list[str] = []
+    for f in sorted(os.listdir(inc)):
+        if not f.endswith(".h"):
+            continue
+        text = open(os.path.join(inc, f)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        text = re.sub(r"//[^\n]*", "", text)
+        for m in re.finditer(r"\b(maxmulsk_[a-z0-9_]+)\s*\(", text):
+            if m.group(1) not in names:
+                names.append(m.group(1))
+    return names
+
+
+__all__ = ["Plan", "Problem", "load", "exported_symbols", "LIB_PATH", "c_float"]

@@ -1,0 +1,93 @@
+// Internal declarations shared by the host runtime and the kernel files.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/maxmulsk.h"
+
+namespace mmsk {
+
+// K is cut into slices of kchunk elements; kchunk is a multiple of this so a
+// slice boundary never splits a staging block of any kernel.
+constexpr int kSliceAlign = 32;
+
+// Slice length for a plan's split_k. The number of slices actually run is
+// ceil(K / kchunk) <= split_k, so no slice is ever empty.
+inline size_t slice_len(size_t K, int split_k) {
+    if (split_k <= 1 || K == 0) return K;
+    size_t per = (K + (size_t)split_k - 1) / (size_t)split_k;
+    per = (per + kSliceAlign - 1) / kSliceAlign * kSliceAlign;
+    return per < K ? per : K;
+}
+inline int slice_count(size_t K, int split_k) {
+    size_t kc = slice_len(K, split_k);
+    return kc ? (int)((K + kc - 1) / kc) : 1;
+}
+
+// Device-side error word bits (one int per device, see runtime.cpp).
+enum : int {
+    kErrTimeout = 1,
+};
+
+// ---------------------------------------------------------------------------
+// SIMT FP32 kernels (simt.cu)
+// ---------------------------------------------------------------------------
+struct SimtArgs {
+    const float* A; const float* B; float* C;
+    int64_t M, K, N;
+    int64_t kchunk;        // slice length (multiple of kSliceAlign) or K
+    int splits;            // slices actually run (>= 1)
+    float* partial;        // splits * M * N floats when splits > 1
+    unsigned* counters;    // one per output tile when splits > 1 (zero on entry)
+};
+// Workspace bytes for the SIMT path with this tile/split choice.
+size_t simt_workspace_bytes(int64_t M, int64_t K, int64_t N, int tile_m, int tile_n, int split_k);
+// Lays out ws into SimtArgs fields. Returns false if ws is too small.
+bool simt_bind_workspace(SimtArgs& a, int tile_m, int tile_n, void* ws, size_t ws_bytes);
+cudaError_t simt_launch(const SimtArgs& a, int tile_m, int tile_n, int variant, cudaStream_t s);
+
+// ---------------------------------------------------------------------------
+// Split-precision tensor-core path (split.cu, tc.cu)
+// ---------------------------------------------------------------------------
+struct TcArgs {
+    const float* A; const float* B; float* C;
+    int64_t M, K, N;
+    int precision;         // MAXMULSK_PREC_3XTF32 / _BF16X6 / _BF16X9
+    int tile_n;            // 64, 128 or 256 (tile_m is 128)
+    bool reuse_planes;     // skip the split pre-pass: planes are already in place
+    int64_t kchunk;
+    int splits;
+    void* planes;          // operand planes written by the split pre-pass
+    float* partial;        // splits * M * N floats when splits > 1
+    unsigned* counters;    // one per output tile when splits > 1
+    int* err;              // device error word
+};
+size_t tc_workspace_bytes(int64_t M, int64_t K, int64_t N, int precision, int tile_n, int split_k);
+bool tc_bind_workspace(TcArgs& a, void* ws, size_t ws_bytes);
+cudaError_t tc_launch(const TcArgs& a, cudaStream_t s);
+
+// Operand plane geometry: A planes are [P][M][Kp] (K-major), B planes are
+// [P][K][Np] (N-major); Kp and Np are padded so rows start on 16-byte (A) and
+// 128-byte (B) boundaries; padding holds zeros.
+struct PlaneGeom {
+    int P;                 // planes per operand: 2 (TF32) or 3 (BF16)
+    int esize;             // bytes per plane element: 4 (TF32) or 2 (BF16)
+    int64_t Kp, Np;
+    size_t a_plane_bytes, b_plane_bytes;   // one plane, rounded to 1 KiB
+};
+PlaneGeom plane_geom(int64_t M, int64_t K, int64_t N, int precision);
+cudaError_t split_launch(const float* A, const float* B, int64_t M, int64_t K, int64_t N,
+                         int precision, void* planes, cudaStream_t s);
+// One matrix, laid out as the A operand (as_b false) or the B operand.
+size_t split_one_bytes(int64_t R, int64_t C, int precision, bool as_b);
+cudaError_t split_one(const float* X, int64_t R, int64_t C, int precision, bool as_b, void* out,
+                      cudaStream_t s);
+
+// Number of SMs of the current device (cached).
+int device_sm_count();
+// Device error word of the current device (allocated on first use).
+int* device_error_word();
+
+}  // namespace mmsk

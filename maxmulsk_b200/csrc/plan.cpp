@@ -1,0 +1,132 @@
+// Plans: validation, workspace sizing, the fixed shape rule and the tuned
+// picker with its environment override.
+//
+// Counterparts in the reference:
+//   classify_plan   NB::classify   sme/v4/sme-1x4-kcout-ncblock-apack4za.cpp:410-423
+//   workspace_bytes NB::capacity   :429-444, v5.1 workspace_bytes (sme/v5/sme-1x4-fusedpack-v51.hpp:75-78)
+//   choose_rule     SMEKernels1x4V4C::choose  sme/v4/sme-1x4-v4c-dispatch.cpp:17-22
+//   choose_tuned    MaxMulSK::tuning::select  sme/support/gemm_tuning.cpp:96-100
+//   parse_config_env parse_env(MAXMULSK_BLOCKING)  sme/support/gemm_tuning.cpp:66-78
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "internal.hpp"
+#include "runtime.hpp"
+#include "tuning.hpp"
+
+namespace mmsk {
+
+namespace {
+bool is_tc(int precision) {
+    return precision == MAXMULSK_PREC_3XTF32 || precision == MAXMULSK_PREC_BF16X6 ||
+           precision == MAXMULSK_PREC_BF16X9;
+}
+constexpr size_t kMaxDim = 0x7FFFFFFFull;   // TMA coordinates and grid sizes are 32-bit
+}  // namespace
+
+maxmulsk_status classify_plan(size_t M, size_t K, size_t N, const maxmulsk_plan* plan) {
+    if (!plan) { set_error_message("null plan"); return MAXMULSK_ERR_INVALID; }
+    const maxmulsk_plan& p = *plan;
+    if (p.split_k < 1 || p.split_k > 64) { set_error_message("split_k must be 1..64"); return MAXMULSK_ERR_UNSUPPORTED; }
+    if (p.precision == MAXMULSK_PREC_FP32) {
+        const bool tile_ok = (p.tile_m == 128 && p.tile_n == 128) || (p.tile_m == 128 && p.tile_n == 64) ||
+                             (p.tile_m == 64 && p.tile_n == 64);
+        if (!tile_ok) { set_error_message("FP32 tiles: 128x128, 128x64 or 64x64"); return MAXMULSK_ERR_UNSUPPORTED; }
+        if (p.variant != MAXMULSK_FP32_FMA && p.variant != MAXMULSK_FP32_SCALAR) {
+            set_error_message("unknown FP32 variant");
+            return MAXMULSK_ERR_UNSUPPORTED;
+        }
+        if (M > kMaxDim || N > kMaxDim || K > kMaxDim) { set_error_message("dimension too large"); return MAXMULSK_ERR_UNSUPPORTED; }
+        if ((M + p.tile_m - 1) / p.tile_m > 65535) { set_error_message("M too large for the FP32 grid"); return MAXMULSK_ERR_UNSUPPORTED; }
+        return MAXMULSK_OK;
+    }
+    if (is_tc(p.precision)) {
+        if (p.tile_m != 128 || (p.tile_n != 64 && p.tile_n != 128 && p.tile_n != 256)) {
+            set_error_message("tensor-core tiles: 128x64, 128x128 or 128x256");
+            return MAXMULSK_ERR_UNSUPPORTED;
+        }
+        if (p.variant != MAXMULSK_TC_SPLIT_INPUTS && p.variant != MAXMULSK_TC_REUSE_PLANES) {
+            set_error_message("unknown tensor-core variant");
+            return MAXMULSK_ERR_UNSUPPORTED;
+        }
+        if (M > kMaxDim || N > kMaxDim || K > kMaxDim) { set_error_message("dimension too large"); return MAXMULSK_ERR_UNSUPPORTED; }
+        return MAXMULSK_OK;
+    }
+    set_error_message("unknown precision");
+    return MAXMULSK_ERR_UNSUPPORTED;
+}
+
+size_t workspace_bytes(size_t M, size_t K, size_t N, const maxmulsk_plan& p) {
+    if (M == 0 || N == 0 || K == 0) return 0;
+    if (p.precision == MAXMULSK_PREC_FP32)
+        return simt_workspace_bytes((int64_t)M, (int64_t)K, (int64_t)N, p.tile_m, p.tile_n, p.split_k);
+    return tc_workspace_bytes((int64_t)M, (int64_t)K, (int64_t)N, p.precision, p.tile_n, p.split_k);
+}
+
+// Two fixed profiles per precision, separated by shape alone, like the v4c
+// rule. A large profile when the output alone fills the machine; otherwise a
+// small tile with K cut into slices until roughly two waves of CTAs exist.
+maxmulsk_plan choose_rule(size_t M, size_t K, size_t N, int precision, int sms) {
+    maxmulsk_plan p;
+    std::memset(&p, 0, sizeof(p));
+    p.precision = precision;
+    p.split_k = 1;
+    if (sms <= 0) sms = 148;
+    if (precision == MAXMULSK_PREC_FP32) {
+        const size_t big_tiles = ((M + 127) / 128) * ((N + 127) / 128);
+        if (big_tiles >= (size_t)sms) {
+            p.tile_m = 128; p.tile_n = 128;
+        } else {
+            p.tile_m = 64; p.tile_n = 64;
+            const size_t tiles = ((M + 63) / 64) * ((N + 63) / 64);
+            size_t want = (2 * (size_t)sms + tiles - 1) / tiles;
+            const size_t kmax = K / 256 ? K / 256 : 1;          // keep slices >= 256 deep
+            if (want > kmax) want = kmax;
+            if (want > 64) want = 64;
+            p.split_k = (int)(want ? want : 1);
+        }
+        return p;
+    }
+    p.tile_m = 128;
+    const size_t t256 = ((M + 127) / 128) * ((N + 255) / 256);
+    const size_t t128 = ((M + 127) / 128) * ((N + 127) / 128);
+    size_t tiles;
+    if (t256 >= (size_t)sms && N >= 256) { p.tile_n = 256; tiles = t256; }
+    else { p.tile_n = 128; tiles = t128; }
+    if (tiles < (size_t)sms) {
+        size_t want = ((size_t)sms + tiles - 1) / tiles;
+        const size_t kmax = K / 512 ? K / 512 : 1;
+        if (want > kmax) want = kmax;
+        if (want > 64) want = 64;
+        p.split_k = (int)(want ? want : 1);
+    }
+    return p;
+}
+
+// MAXMULSK_CONFIG="precision,tile_m,tile_n,split_k[,variant]" overrides the
+// picker; malformed values are ignored, as the reference's parse_env does.
+bool parse_config_env(maxmulsk_plan& out) {
+    const char* s = std::getenv("MAXMULSK_CONFIG");
+    if (!s || !*s) return false;
+    int prec = 0, tm = 0, tn = 0, sk = 0, var = 0;
+    const int n = std::sscanf(s, "%d,%d,%d,%d,%d", &prec, &tm, &tn, &sk, &var);
+    if (n != 4 && n != 5) return false;
+    if (tm <= 0 || tn <= 0 || sk <= 0) return false;
+    maxmulsk_plan p;
+    std::memset(&p, 0, sizeof(p));
+    p.precision = prec; p.tile_m = tm; p.tile_n = tn; p.split_k = sk; p.variant = (n == 5) ? var : 0;
+    out = p;
+    return true;
+}
+
+// Tuning database entry for this exact shape, else the learned cost model,
+// else the rule.
+maxmulsk_plan choose_tuned(size_t M, size_t K, size_t N, int precision, int sms) {
+    maxmulsk_plan p;
+    if (tuning_lookup(M, K, N, precision, &p)) return p;
+    if (tuning_predict(M, K, N, precision, &p)) return p;
+    return choose_rule(M, K, N, precision, sms);
+}
+
+}  // namespace mmsk

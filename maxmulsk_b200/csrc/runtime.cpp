@@ -1,0 +1,249 @@
+// Host runtime: device state, workspace cache, host staging and dispatch.
+//
+// The reference allocates its packing buffers inside every call and frees
+// them on return (sme/v3/sme-1x4-acc-kcout.cpp:455-461,
+// sme/v4/sme-1x4-kcout-ncblock-apack4za.cpp:638-654). On the GPU that would
+// cost a cudaMalloc/cudaFree pair per call, so workspace here is cached per
+// (device, stream) and only ever grows; the host-pointer entry points also
+// keep per-thread device copies of A, B and C.
+#include "runtime.hpp"
+
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "internal.hpp"
+
+namespace mmsk {
+
+// ------------------------------------------------------------------ errors
+namespace {
+thread_local std::string t_last_error;
+}
+void set_error_message(const std::string& msg) { t_last_error = msg; }
+const char* last_error_message() { return t_last_error.c_str(); }
+
+maxmulsk_status cuda_status(cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return MAXMULSK_OK;
+    set_error_message(std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")");
+    if (e == cudaErrorMemoryAllocation) return MAXMULSK_ERR_ALLOC;
+    return MAXMULSK_ERR_CUDA;
+}
+
+// ------------------------------------------------------------------ devices
+namespace {
+
+struct Workspace {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct DeviceState {
+    int sms = 0;
+    int major = 0, minor = 0;
+    int* err_word = nullptr;
+    std::mutex mu;
+    std::map<cudaStream_t, Workspace> ws;
+};
+
+std::mutex g_devices_mu;
+std::vector<std::unique_ptr<DeviceState>> g_devices;
+
+DeviceState* device_state(int dev) {
+    std::lock_guard<std::mutex> lk(g_devices_mu);
+    if ((int)g_devices.size() <= dev) g_devices.resize(dev + 1);
+    if (!g_devices[dev]) {
+        auto st = std::make_unique<DeviceState>();
+        cudaDeviceGetAttribute(&st->sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaDeviceGetAttribute(&st->major, cudaDevAttrComputeCapabilityMajor, dev);
+        cudaDeviceGetAttribute(&st->minor, cudaDevAttrComputeCapabilityMinor, dev);
+        if (cudaMalloc(&st->err_word, sizeof(int)) == cudaSuccess) cudaMemset(st->err_word, 0, sizeof(int));
+        else st->err_word = nullptr;
+        g_devices[dev] = std::move(st);
+    }
+    return g_devices[dev].get();
+}
+
+DeviceState* current_state() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return device_state(dev);
+}
+
+// Per-thread device copies for the host-pointer entry points.
+struct HostStage {
+    cudaStream_t stream = nullptr;
+    float* dA = nullptr; size_t capA = 0;
+    float* dB = nullptr; size_t capB = 0;
+    float* dC = nullptr; size_t capC = 0;
+};
+thread_local std::map<int, HostStage> t_stage;
+
+cudaError_t grow(float** p, size_t* cap, size_t need_elems) {
+    if (*cap >= need_elems) return cudaSuccess;
+    if (*p) cudaFree(*p);
+    *p = nullptr; *cap = 0;
+    cudaError_t e = cudaMalloc(p, need_elems * sizeof(float));
+    if (e == cudaSuccess) *cap = need_elems;
+    return e;
+}
+
+}  // namespace
+
+int device_sm_count() { return current_state()->sms; }
+int* device_error_word() { return current_state()->err_word; }
+
+// ------------------------------------------------------------------ dispatch
+bool handle_empty_dev(float* dC, size_t M, size_t K, size_t N, cudaStream_t s, maxmulsk_status* st) {
+    if (M == 0 || N == 0) { *st = MAXMULSK_OK; return true; }
+    if (K == 0) {
+        *st = cuda_status(cudaMemsetAsync(dC, 0, M * N * sizeof(float), s), "cudaMemsetAsync(C)");
+        return true;
+    }
+    return false;
+}
+
+maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
+                             const maxmulsk_plan& plan, void* ws, size_t ws_bytes, cudaStream_t s) {
+    maxmulsk_status st = classify_plan(M, K, N, &plan);
+    if (st != MAXMULSK_OK) return st;
+    if (handle_empty_dev(dC, M, K, N, s, &st)) return st;
+    if (!dA || !dB || !dC) { set_error_message("null matrix pointer"); return MAXMULSK_ERR_INVALID; }
+    const size_t need = workspace_bytes(M, K, N, plan);
+    if (need > 0 && (!ws || ws_bytes < need || (reinterpret_cast<uintptr_t>(ws) & 255) != 0)) {
+        set_error_message("workspace missing, too small or not 256-byte aligned");
+        return MAXMULSK_ERR_INVALID;
+    }
+    DeviceState* ds = current_state();
+    if (!ds->err_word) { set_error_message("device error word unavailable"); return MAXMULSK_ERR_ALLOC; }
+
+    if (plan.precision == MAXMULSK_PREC_FP32) {
+        SimtArgs a{};
+        a.A = dA; a.B = dB; a.C = dC;
+        a.M = (int64_t)M; a.K = (int64_t)K; a.N = (int64_t)N;
+        a.kchunk = (int64_t)slice_len(K, plan.split_k);
+        a.splits = slice_count(K, plan.split_k);
+        if (!simt_bind_workspace(a, plan.tile_m, plan.tile_n, ws, ws_bytes)) {
+            set_error_message("workspace too small for the SIMT plan");
+            return MAXMULSK_ERR_INVALID;
+        }
+        if (a.splits > 1) {
+            const size_t tiles = (size_t)((M + plan.tile_m - 1) / plan.tile_m) * ((N + plan.tile_n - 1) / plan.tile_n);
+            st = cuda_status(cudaMemsetAsync(a.counters, 0, tiles * sizeof(unsigned), s), "cudaMemsetAsync(counters)");
+            if (st != MAXMULSK_OK) return st;
+        }
+        return cuda_status(simt_launch(a, plan.tile_m, plan.tile_n, plan.variant, s), "sgemm_simt launch");
+    }
+
+    if (ds->major != 10) {
+        set_error_message("split-precision tensor-core kernels need an sm_100 device");
+        return MAXMULSK_ERR_UNSUPPORTED;
+    }
+    TcArgs a{};
+    a.A = dA; a.B = dB; a.C = dC;
+    a.M = (int64_t)M; a.K = (int64_t)K; a.N = (int64_t)N;
+    a.precision = plan.precision;
+    a.tile_n = plan.tile_n;
+    a.reuse_planes = (plan.variant == MAXMULSK_TC_REUSE_PLANES);
+    a.kchunk = (int64_t)slice_len(K, plan.split_k);
+    a.splits = slice_count(K, plan.split_k);
+    a.err = ds->err_word;
+    if (!tc_bind_workspace(a, ws, ws_bytes)) {
+        set_error_message("workspace too small for the tensor-core plan");
+        return MAXMULSK_ERR_INVALID;
+    }
+    if (a.splits > 1) {
+        const size_t tiles = (size_t)((M + 127) / 128) * ((N + plan.tile_n - 1) / plan.tile_n);
+        st = cuda_status(cudaMemsetAsync(a.counters, 0, tiles * 4 * sizeof(unsigned), s), "cudaMemsetAsync(counters)");
+        if (st != MAXMULSK_OK) return st;
+    }
+    return cuda_status(tc_launch(a, s), "sgemm_split_tc launch");
+}
+
+maxmulsk_status run_plan_managed(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
+                                 const maxmulsk_plan& plan, cudaStream_t s) {
+    maxmulsk_status st = classify_plan(M, K, N, &plan);
+    if (st != MAXMULSK_OK) return st;
+    if (handle_empty_dev(dC, M, K, N, s, &st)) return st;
+    const size_t need = workspace_bytes(M, K, N, plan);
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    if (need > 0) {
+        DeviceState* ds = current_state();
+        std::lock_guard<std::mutex> lk(ds->mu);
+        Workspace& w = ds->ws[s];
+        if (w.bytes < need) {
+            // The old buffer may still be read by work queued on this stream.
+            if (w.ptr) {
+                st = cuda_status(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+                if (st != MAXMULSK_OK) return st;
+                cudaFree(w.ptr);
+                w.ptr = nullptr;
+                w.bytes = 0;
+            }
+            size_t grown = need + need / 4;
+            cudaError_t e = cudaMalloc(&w.ptr, grown);
+            if (e != cudaSuccess) {
+                w.ptr = nullptr;
+                return cuda_status(e, "cudaMalloc(workspace)");
+            }
+            w.bytes = grown;
+        }
+        ws = w.ptr;
+        ws_bytes = w.bytes;
+    }
+    return run_plan_dev(dA, dB, dC, M, K, N, plan, ws, ws_bytes, s);
+}
+
+maxmulsk_status stream_status(cudaStream_t s) {
+    maxmulsk_status st = cuda_status(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+    if (st != MAXMULSK_OK) return st;
+    DeviceState* ds = current_state();
+    if (!ds->err_word) return MAXMULSK_OK;
+    int flag = 0;
+    st = cuda_status(cudaMemcpy(&flag, ds->err_word, sizeof(int), cudaMemcpyDeviceToHost), "read error word");
+    if (st != MAXMULSK_OK) return st;
+    if (flag != 0) {
+        cudaMemset(ds->err_word, 0, sizeof(int));
+        set_error_message("a bounded device-side wait timed out");
+        return MAXMULSK_ERR_TIMEOUT;
+    }
+    return MAXMULSK_OK;
+}
+
+maxmulsk_status run_plan_host(const float* A, const float* B, float* C, size_t M, size_t K, size_t N,
+                              const maxmulsk_plan& plan) {
+    maxmulsk_status st = classify_plan(M, K, N, &plan);
+    if (st != MAXMULSK_OK) return st;
+    if (M == 0 || N == 0) return MAXMULSK_OK;
+    if (!C) { set_error_message("null C"); return MAXMULSK_ERR_INVALID; }
+    if (K == 0) { std::memset(C, 0, M * N * sizeof(float)); return MAXMULSK_OK; }
+    if (!A || !B) { set_error_message("null A or B"); return MAXMULSK_ERR_INVALID; }
+
+    int dev = 0;
+    st = cuda_status(cudaGetDevice(&dev), "cudaGetDevice");
+    if (st != MAXMULSK_OK) return st;
+    HostStage& hs = t_stage[dev];
+    if (!hs.stream) {
+        st = cuda_status(cudaStreamCreateWithFlags(&hs.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        if (st != MAXMULSK_OK) return st;
+    }
+    if ((st = cuda_status(grow(&hs.dA, &hs.capA, M * K), "cudaMalloc(A)")) != MAXMULSK_OK) return st;
+    if ((st = cuda_status(grow(&hs.dB, &hs.capB, K * N), "cudaMalloc(B)")) != MAXMULSK_OK) return st;
+    if ((st = cuda_status(grow(&hs.dC, &hs.capC, M * N), "cudaMalloc(C)")) != MAXMULSK_OK) return st;
+
+    cudaStream_t s = hs.stream;
+    st = cuda_status(cudaMemcpyAsync(hs.dA, A, M * K * sizeof(float), cudaMemcpyHostToDevice, s), "copy A");
+    if (st != MAXMULSK_OK) return st;
+    st = cuda_status(cudaMemcpyAsync(hs.dB, B, K * N * sizeof(float), cudaMemcpyHostToDevice, s), "copy B");
+    if (st != MAXMULSK_OK) return st;
+    st = run_plan_managed(hs.dA, hs.dB, hs.dC, M, K, N, plan, s);
+    if (st != MAXMULSK_OK) { cudaStreamSynchronize(s); return st; }
+    st = cuda_status(cudaMemcpyAsync(C, hs.dC, M * N * sizeof(float), cudaMemcpyDeviceToHost, s), "copy C");
+    if (st != MAXMULSK_OK) { cudaStreamSynchronize(s); return st; }
+    return stream_status(s);
+}
+
+}  // namespace mmsk

@@ -1,0 +1,46 @@
+// Host runtime: per-device state, workspace cache, per-thread host staging,
+// plan validation and dispatch. C++ only; the C ABI in capi.cpp wraps it.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+
+#include "../../include/maxmulsk.h"
+
+namespace mmsk {
+
+// Records a CUDA error message for maxmulsk_last_error_message() and maps it
+// to a status (allocation failures to MAXMULSK_ERR_ALLOC).
+maxmulsk_status cuda_status(cudaError_t e, const char* where);
+void set_error_message(const std::string& msg);
+const char* last_error_message();
+
+// Plan helpers (plan.cpp).
+maxmulsk_status classify_plan(size_t M, size_t K, size_t N, const maxmulsk_plan* plan);
+size_t workspace_bytes(size_t M, size_t K, size_t N, const maxmulsk_plan& plan);
+maxmulsk_plan choose_rule(size_t M, size_t K, size_t N, int precision, int sms);
+maxmulsk_plan choose_tuned(size_t M, size_t K, size_t N, int precision, int sms);
+bool parse_config_env(maxmulsk_plan& out);
+
+// Runs a validated plan on device pointers with a caller-provided workspace.
+maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
+                             const maxmulsk_plan& plan, void* ws, size_t ws_bytes, cudaStream_t s);
+
+// Runs a plan with the library-managed workspace of (current device, stream).
+maxmulsk_status run_plan_managed(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
+                                 const maxmulsk_plan& plan, cudaStream_t s);
+
+// Host-pointer form: copy in, run, copy out, wait, check the error word.
+maxmulsk_status run_plan_host(const float* A, const float* B, float* C, size_t M, size_t K, size_t N,
+                              const maxmulsk_plan& plan);
+
+// Empty-shape contract of the reference (capi/maxmulsk.cpp:13-20), on device
+// memory: true when handled. K == 0 zeroes C.
+bool handle_empty_dev(float* dC, size_t M, size_t K, size_t N, cudaStream_t s, maxmulsk_status* st);
+
+// Waits for `s`, then reports and clears the device error word.
+maxmulsk_status stream_status(cudaStream_t s);
+
+}  // namespace mmsk

@@ -1,0 +1,283 @@
+// FP32 SIMT GEMM for sm_100a: C = A*B, row-major, on the CUDA cores.
+//
+// Replaces the reference's blocked SME driver (sme/v3/sme-1x4-acc-kcout.cpp:427-567)
+// as the FP32-accurate path. The SME packers (pack_A_streaming :39-136 with
+// its ZA transpose, pack_B_streaming :145-193) become shared-memory staging:
+// A is stored k-major (transposed on the way in, like the ZA transpose), B
+// row-major; both double-buffered, fed by 128-bit global loads. The 16x64 ZA
+// micro-tile becomes a CTA tile of tile_m x tile_n with an 8x8 (or 4x4)
+// register tile per thread.
+//
+// Arithmetic: every output is ONE sequential chain over k in increasing order
+// (a fused multiply-add per step, or multiply-then-add in the SCALAR variant,
+// the arithmetic of Utils::multiply_scalar, common/utils.hpp:50-61). With
+// split_k > 1 each K slice is such a chain and the slices are summed in slice
+// order, first slice first: C = ((p0 + p1) + p2) + ..., the order in which
+// the reference's v3 adds its outer-Kc panels (first_k store, then
+// store_za_add; sme/v3/sme-1x4-acc-kcout.cpp:464-471, 530-558). The result is
+// therefore deterministic and reproducible bit for bit by a scalar loop.
+//
+// Edges (the reference's scratch-tile path, :539-558) are predicated loads
+// that read zero outside the matrix and predicated stores; C outside the
+// matrix is never touched.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "internal.hpp"
+
+namespace mmsk {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kBK = 16;
+
+template <bool FUSED>
+__device__ __forceinline__ float mac(float a, float b, float c) {
+    if constexpr (FUSED) return __fmaf_rn(a, b, c);
+    else return __fadd_rn(c, __fmul_rn(a, b));
+}
+
+// One CTA computes a BM x BN tile of one K slice (blockIdx.z).
+template <int BM, int BN, bool FUSED, bool VEC>
+__global__ void __launch_bounds__(kThreads, 2)
+sgemm_simt_kernel(SimtArgs p) {
+    constexpr int TM = BM / 16, TN = BN / 16;       // per-thread outputs
+    constexpr int GM = TM / 4, GN = TN / 4;         // 4-wide groups per thread
+    constexpr int A_F4 = BM * kBK / 4 / kThreads;   // float4 loads per thread
+    constexpr int B_F4 = BN * kBK / 4 / kThreads;
+    constexpr int AP = BM + 4;                      // padded row of the k-major A stage
+
+    __shared__ __align__(16) float As[2][kBK][AP];
+    __shared__ __align__(16) float Bs[2][kBK][BN];
+
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+    const int64_t m0 = (int64_t)blockIdx.y * BM;
+    const int64_t n0 = (int64_t)blockIdx.x * BN;
+    const int z = blockIdx.z;
+    const int64_t kbeg = (int64_t)z * p.kchunk;
+    const int64_t kend = min(p.K, kbeg + p.kchunk);
+    const int64_t M = p.M, N = p.N, K = p.K;
+    const float* __restrict__ A = p.A;
+    const float* __restrict__ B = p.B;
+
+    float4 ra[A_F4], rb[B_F4];
+
+    auto load_tile = [&](int64_t k0) {
+#pragma unroll
+        for (int j = 0; j < A_F4; j++) {
+            const int f = tid + j * kThreads;
+            const int row = f / (kBK / 4);
+            const int kq = (f % (kBK / 4)) * 4;
+            const int64_t gm = m0 + row, gk = k0 + kq;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (gm < M) {
+                const float* src = A + gm * K + gk;
+                if (VEC) {
+                    if (gk < kend) v = __ldg(reinterpret_cast<const float4*>(src));
+                } else {
+                    if (gk + 0 < kend) v.x = __ldg(src + 0);
+                    if (gk + 1 < kend) v.y = __ldg(src + 1);
+                    if (gk + 2 < kend) v.z = __ldg(src + 2);
+                    if (gk + 3 < kend) v.w = __ldg(src + 3);
+                }
+            }
+            ra[j] = v;
+        }
+#pragma unroll
+        for (int j = 0; j < B_F4; j++) {
+            const int f = tid + j * kThreads;
+            const int kr = f / (BN / 4);
+            const int nq = (f % (BN / 4)) * 4;
+            const int64_t gk = k0 + kr, gn = n0 + nq;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (gk < kend) {
+                const float* src = B + gk * N + gn;
+                if (VEC) {
+                    if (gn < N) v = __ldg(reinterpret_cast<const float4*>(src));
+                } else {
+                    if (gn + 0 < N) v.x = __ldg(src + 0);
+                    if (gn + 1 < N) v.y = __ldg(src + 1);
+                    if (gn + 2 < N) v.z = __ldg(src + 2);
+                    if (gn + 3 < N) v.w = __ldg(src + 3);
+                }
+            }
+            rb[j] = v;
+        }
+    };
+    auto store_tile = [&](int buf) {
+#pragma unroll
+        for (int j = 0; j < A_F4; j++) {
+            const int f = tid + j * kThreads;
+            const int row = f / (kBK / 4);
+            const int kq = (f % (kBK / 4)) * 4;
+            As[buf][kq + 0][row] = ra[j].x;
+            As[buf][kq + 1][row] = ra[j].y;
+            As[buf][kq + 2][row] = ra[j].z;
+            As[buf][kq + 3][row] = ra[j].w;
+        }
+#pragma unroll
+        for (int j = 0; j < B_F4; j++) {
+            const int f = tid + j * kThreads;
+            const int kr = f / (BN / 4);
+            const int nq = (f % (BN / 4)) * 4;
+            *reinterpret_cast<float4*>(&Bs[buf][kr][nq]) = rb[j];
+        }
+    };
+
+    float acc[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; i++)
+#pragma unroll
+        for (int j = 0; j < TN; j++) acc[i][j] = 0.f;
+
+    const int64_t ntiles = (kend - kbeg + kBK - 1) / kBK;
+    if (ntiles > 0) {
+        load_tile(kbeg);
+        store_tile(0);
+        __syncthreads();
+        for (int64_t t = 0; t < ntiles; t++) {
+            const int buf = (int)(t & 1);
+            if (t + 1 < ntiles) load_tile(kbeg + (t + 1) * kBK);
+#pragma unroll
+            for (int k = 0; k < kBK; k++) {
+                float a[TM], b[TN];
+#pragma unroll
+                for (int g = 0; g < GM; g++) {
+                    float4 v = *reinterpret_cast<const float4*>(&As[buf][k][g * 64 + ty * 4]);
+                    a[g * 4 + 0] = v.x; a[g * 4 + 1] = v.y; a[g * 4 + 2] = v.z; a[g * 4 + 3] = v.w;
+                }
+#pragma unroll
+                for (int g = 0; g < GN; g++) {
+                    float4 v = *reinterpret_cast<const float4*>(&Bs[buf][k][g * 64 + tx * 4]);
+                    b[g * 4 + 0] = v.x; b[g * 4 + 1] = v.y; b[g * 4 + 2] = v.z; b[g * 4 + 3] = v.w;
+                }
+#pragma unroll
+                for (int i = 0; i < TM; i++)
+#pragma unroll
+                    for (int j = 0; j < TN; j++) acc[i][j] = mac<FUSED>(a[i], b[j], acc[i][j]);
+            }
+            if (t + 1 < ntiles) store_tile(buf ^ 1);
+            __syncthreads();
+        }
+    }
+
+    // Steps past kend multiply by a zero operand. The product is +-0 and adding
+    // it leaves the chain unchanged (the chain never holds -0: it starts at +0
+    // and an exact zero sum rounds to +0), so the padded steps keep the result
+    // identical to a chain over [kbeg, kend) alone.
+
+    auto out_row = [&](int i) { return m0 + (i / 4) * 64 + ty * 4 + (i % 4); };
+    auto out_col = [&](int g) { return n0 + g * 64 + tx * 4; };
+
+    if (p.splits <= 1) {
+#pragma unroll
+        for (int i = 0; i < TM; i++) {
+            const int64_t r = out_row(i);
+            if (r >= M) continue;
+#pragma unroll
+            for (int g = 0; g < GN; g++) {
+                const int64_t c = out_col(g);
+                float* dst = p.C + r * N + c;
+                if (VEC && c + 3 < N) {
+                    *reinterpret_cast<float4*>(dst) =
+                        make_float4(acc[i][g * 4 + 0], acc[i][g * 4 + 1], acc[i][g * 4 + 2], acc[i][g * 4 + 3]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+                        if (c + j < N) dst[j] = acc[i][g * 4 + j];
+                }
+            }
+        }
+        return;
+    }
+
+    // Split-K: write this slice's partial tile, then the last CTA of the tile
+    // to arrive sums all slices in slice order.
+    const size_t MN = (size_t)M * (size_t)N;
+    float* mine = p.partial + (size_t)z * MN;
+#pragma unroll
+    for (int i = 0; i < TM; i++) {
+        const int64_t r = out_row(i);
+        if (r >= M) continue;
+#pragma unroll
+        for (int g = 0; g < GN; g++) {
+            const int64_t c = out_col(g);
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (c + j < N) __stcg(mine + r * N + c + j, acc[i][g * 4 + j]);
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    __shared__ int s_last;
+    const unsigned tile = blockIdx.y * gridDim.x + blockIdx.x;
+    if (tid == 0) {
+        unsigned prev = atomicAdd(&p.counters[tile], 1u);
+        s_last = (prev == (unsigned)(p.splits - 1));
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+#pragma unroll
+    for (int i = 0; i < TM; i++) {
+        const int64_t r = out_row(i);
+        if (r >= M) continue;
+#pragma unroll
+        for (int g = 0; g < GN; g++) {
+            const int64_t c = out_col(g);
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (c + j >= N) continue;
+                const size_t off = (size_t)r * N + c + j;
+                float s = __ldcg(p.partial + off);
+                for (int q = 1; q < p.splits; q++) s = __fadd_rn(s, __ldcg(p.partial + (size_t)q * MN + off));
+                p.C[off] = s;
+            }
+        }
+    }
+    if (tid == 0) p.counters[tile] = 0u;   // leave the counter ready for the next call
+}
+
+template <int BM, int BN>
+cudaError_t launch_tile(const SimtArgs& a, int variant, cudaStream_t s) {
+    dim3 grid((unsigned)((a.N + BN - 1) / BN), (unsigned)((a.M + BM - 1) / BM), (unsigned)a.splits);
+    const bool vec = (a.K % 4 == 0) && (a.N % 4 == 0) &&
+                     ((uintptr_t)a.A % 16 == 0) && ((uintptr_t)a.B % 16 == 0) && ((uintptr_t)a.C % 16 == 0);
+    const bool fused = (variant != MAXMULSK_FP32_SCALAR);
+    if (fused && vec) sgemm_simt_kernel<BM, BN, true, true><<<grid, kThreads, 0, s>>>(a);
+    else if (fused) sgemm_simt_kernel<BM, BN, true, false><<<grid, kThreads, 0, s>>>(a);
+    else if (vec) sgemm_simt_kernel<BM, BN, false, true><<<grid, kThreads, 0, s>>>(a);
+    else sgemm_simt_kernel<BM, BN, false, false><<<grid, kThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+}  // namespace
+
+size_t simt_workspace_bytes(int64_t M, int64_t K, int64_t N, int tile_m, int tile_n, int split_k) {
+    const int splits = slice_count((size_t)K, split_k);
+    if (splits <= 1) return 0;
+    const size_t tiles = (size_t)((M + tile_m - 1) / tile_m) * (size_t)((N + tile_n - 1) / tile_n);
+    return align256(tiles * sizeof(unsigned)) + align256((size_t)splits * (size_t)M * (size_t)N * sizeof(float));
+}
+
+bool simt_bind_workspace(SimtArgs& a, int tile_m, int tile_n, void* ws, size_t ws_bytes) {
+    if (a.splits <= 1) { a.partial = nullptr; a.counters = nullptr; return true; }
+    const size_t tiles = (size_t)((a.M + tile_m - 1) / tile_m) * (size_t)((a.N + tile_n - 1) / tile_n);
+    const size_t need = align256(tiles * sizeof(unsigned)) + align256((size_t)a.splits * a.M * a.N * sizeof(float));
+    if (!ws || ws_bytes < need) return false;
+    a.counters = static_cast<unsigned*>(ws);
+    a.partial = reinterpret_cast<float*>(static_cast<char*>(ws) + align256(tiles * sizeof(unsigned)));
+    return true;
+}
+
+cudaError_t simt_launch(const SimtArgs& a, int tile_m, int tile_n, int variant, cudaStream_t s) {
+    if (tile_m == 128 && tile_n == 128) return launch_tile<128, 128>(a, variant, s);
+    if (tile_m == 128 && tile_n == 64) return launch_tile<128, 64>(a, variant, s);
+    if (tile_m == 64 && tile_n == 64) return launch_tile<64, 64>(a, variant, s);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace mmsk

@@ -1,0 +1,167 @@
+// Split pre-pass: FP32 operands -> tensor-core operand planes.
+//
+// Replaces the reference's packers (pack_A_streaming / pack_B_streaming,
+// sme/v3/sme-1x4-acc-kcout.cpp:39-193) for the split-precision path. A is
+// written K-major as [P][M][Kp]. B is written N-major in 128-byte column
+// panels, [P][Np/NBE][K][NBE] with NBE = 128 bytes of elements, the GPU
+// counterpart of the reference's 64-column B panels
+// (packed_B[g*K_curr*64 + k*64 + c], :145-193). Padding is zero, so it
+// contributes nothing, like the reference's zero-padded edge packs.
+//
+// Planes, from their definitions (finite inputs):
+//   3xTF32 : hi = rna_tf32(x), lo = rna_tf32(x - hi)   (P = 2, stored as FP32
+//            bit patterns with the low 13 mantissa bits clear)
+//   BF16x6 / BF16x9 : l0 = rne_bf16(x), l1 = rne_bf16(x - l0),
+//            l2 = rne_bf16(x - l0 - l1)                  (P = 3, stored as BF16)
+// x - hi and x - l0 - l1 are exact in FP32 (Sterbenz), so hi + lo and
+// l0 + l1 + l2 represent x to 2^-22 and 2^-24 relative respectively.
+//
+// HBM-bound: one read of each operand, P writes.
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "internal.hpp"
+
+namespace mmsk {
+namespace {
+
+// Round to TF32 (10 explicit mantissa bits), nearest, ties away from zero:
+// add half an ulp to the magnitude bits and clear the 13 dropped bits.
+__device__ __forceinline__ float tf32_rna(float x) {
+    uint32_t b = __float_as_uint(x);
+    return __uint_as_float((b + 0x1000u) & 0xFFFFE000u);
+}
+
+// Round to BF16, nearest, ties to even; returned as the 16 stored bits.
+__device__ __forceinline__ uint16_t bf16_rne_bits(float x) {
+    uint32_t b = __float_as_uint(x);
+    return (uint16_t)((b + 0x7FFFu + ((b >> 16) & 1u)) >> 16);
+}
+__device__ __forceinline__ float bf16_bits_to_float(uint16_t h) { return __uint_as_float((uint32_t)h << 16); }
+
+// One pass over a row-major R x Cin FP32 matrix, writing P planes of R x Cout
+// (Cout >= Cin, multiple of 4; columns >= Cin are zero). Each thread handles 4
+// consecutive output columns. With panel > 0 the plane is stored in column
+// panels of `panel` elements: element (r, c) at ((c / panel) * R + r) * panel
+// + c % panel; with panel == 0 it is stored row-major.
+template <int MODE>
+__global__ void __launch_bounds__(256)
+split_kernel(const float* __restrict__ src, int64_t R, int64_t Cin, int64_t Cout, int64_t panel,
+             void* __restrict__ planes, size_t plane_bytes) {
+    const int64_t quads_per_row = Cout / 4;
+    const int64_t total = R * quads_per_row;
+    const bool vec = (Cin % 4 == 0) && (((uintptr_t)src & 15) == 0);
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = q / quads_per_row;
+        const int64_t c = (q % quads_per_row) * 4;
+        float x[4];
+        const float* row = src + r * Cin;
+        if (vec && c + 3 < Cin) {
+            float4 v = __ldcs(reinterpret_cast<const float4*>(row + c));
+            x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) x[j] = (c + j < Cin) ? __ldcs(row + c + j) : 0.0f;
+        }
+        const size_t off = panel > 0
+            ? ((size_t)(c / panel) * (size_t)R + (size_t)r) * (size_t)panel + (size_t)(c % panel)
+            : (size_t)r * (size_t)Cout + (size_t)c;
+        if constexpr (MODE == MAXMULSK_PREC_3XTF32) {
+            float hi[4], lo[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                hi[j] = tf32_rna(x[j]);
+                lo[j] = tf32_rna(x[j] - hi[j]);
+            }
+            float* p0 = reinterpret_cast<float*>(planes);
+            float* p1 = reinterpret_cast<float*>(reinterpret_cast<char*>(planes) + plane_bytes);
+            *reinterpret_cast<float4*>(p0 + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<float4*>(p1 + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+        } else {
+            uint16_t l[3][4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const uint16_t a = bf16_rne_bits(x[j]);
+                const float r1 = x[j] - bf16_bits_to_float(a);
+                const uint16_t b = bf16_rne_bits(r1);
+                const float r2 = r1 - bf16_bits_to_float(b);
+                l[0][j] = a; l[1][j] = b; l[2][j] = bf16_rne_bits(r2);
+            }
+#pragma unroll
+            for (int p = 0; p < 3; p++) {
+                uint16_t* dst = reinterpret_cast<uint16_t*>(reinterpret_cast<char*>(planes) + (size_t)p * plane_bytes);
+                uint2 packed;
+                packed.x = (uint32_t)l[p][0] | ((uint32_t)l[p][1] << 16);
+                packed.y = (uint32_t)l[p][2] | ((uint32_t)l[p][3] << 16);
+                *reinterpret_cast<uint2*>(dst + off) = packed;
+            }
+        }
+    }
+}
+
+inline size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+template <int MODE>
+cudaError_t launch_one(const float* src, int64_t R, int64_t Cin, int64_t Cout, int64_t panel,
+                       void* planes, size_t plane_bytes, cudaStream_t s) {
+    const int64_t total = R * (Cout / 4);
+    if (total == 0) return cudaSuccess;
+    const int sms = device_sm_count();
+    int64_t blocks = (total + 255) / 256;
+    const int64_t cap = (int64_t)sms * 8;
+    if (blocks > cap) blocks = cap;
+    split_kernel<MODE><<<(unsigned)blocks, 256, 0, s>>>(src, R, Cin, Cout, panel, planes, plane_bytes);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+PlaneGeom plane_geom(int64_t M, int64_t K, int64_t N, int precision) {
+    PlaneGeom g;
+    const bool tf32 = (precision == MAXMULSK_PREC_3XTF32);
+    g.P = tf32 ? 2 : 3;
+    g.esize = tf32 ? 4 : 2;
+    // A rows: a multiple of 16 bytes (TMA row stride). B: a whole number of
+    // 128-byte column panels.
+    g.Kp = (int64_t)round_up((size_t)K, (size_t)(16 / g.esize));
+    g.Np = (int64_t)round_up((size_t)N, (size_t)(128 / g.esize));
+    g.a_plane_bytes = round_up((size_t)M * (size_t)g.Kp * (size_t)g.esize, 1024);
+    g.b_plane_bytes = round_up((size_t)K * (size_t)g.Np * (size_t)g.esize, 1024);
+    return g;
+}
+
+cudaError_t split_launch(const float* A, const float* B, int64_t M, int64_t K, int64_t N,
+                         int precision, void* planes, cudaStream_t s) {
+    const PlaneGeom g = plane_geom(M, K, N, precision);
+    char* a_planes = static_cast<char*>(planes);
+    char* b_planes = a_planes + (size_t)g.P * g.a_plane_bytes;
+    cudaError_t e;
+    if (precision == MAXMULSK_PREC_3XTF32) {
+        e = launch_one<MAXMULSK_PREC_3XTF32>(A, M, K, g.Kp, 0, a_planes, g.a_plane_bytes, s);
+        if (e != cudaSuccess) return e;
+        return launch_one<MAXMULSK_PREC_3XTF32>(B, K, N, g.Np, 128 / g.esize, b_planes, g.b_plane_bytes, s);
+    }
+    e = launch_one<MAXMULSK_PREC_BF16X6>(A, M, K, g.Kp, 0, a_planes, g.a_plane_bytes, s);
+    if (e != cudaSuccess) return e;
+    return launch_one<MAXMULSK_PREC_BF16X6>(B, K, N, g.Np, 128 / g.esize, b_planes, g.b_plane_bytes, s);
+}
+
+size_t split_one_bytes(int64_t R, int64_t C, int precision, bool as_b) {
+    // As A: R x C is M x K. As B: R x C is K x N.
+    const PlaneGeom g = as_b ? plane_geom(1, R, C, precision) : plane_geom(R, C, 1, precision);
+    return (size_t)g.P * (as_b ? g.b_plane_bytes : g.a_plane_bytes);
+}
+
+cudaError_t split_one(const float* X, int64_t R, int64_t C, int precision, bool as_b, void* out,
+                      cudaStream_t s) {
+    const PlaneGeom g = as_b ? plane_geom(1, R, C, precision) : plane_geom(R, C, 1, precision);
+    const int64_t cout = as_b ? g.Np : g.Kp;
+    const int64_t panel = as_b ? 128 / g.esize : 0;
+    const size_t pb = as_b ? g.b_plane_bytes : g.a_plane_bytes;
+    if (precision == MAXMULSK_PREC_3XTF32)
+        return launch_one<MAXMULSK_PREC_3XTF32>(X, R, C, cout, panel, out, pb, s);
+    return launch_one<MAXMULSK_PREC_BF16X6>(X, R, C, cout, panel, out, pb, s);
+}
+
+}  // namespace mmsk

@@ -1,0 +1,96 @@
+"""The C-ABI library without a GPU: it loads, exports every symbol the
+headers declare, and its pure host logic (plan validation, workspace sizing,
+status names) behaves. No compute call is made here."""
+import ctypes
+import subprocess
+
+import pytest
+
+import maxmulsk_b200 as mm
+from maxmulsk_b200 import _lib
+
+
+def test_library_exports_every_declared_symbol(built_lib):
+    declared = _lib.exported_symbols()
+    assert "maxmulsk_sgemm_v3" in declared and "maxmulsk_sgemm_v4" in declared
+    missing = [n for n in declared if not hasattr(built_lib, n)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    for n in declared:
+        assert f" T {n}" in out, n
+
+
+def test_binding_table_covers_header(built_lib):
+    assert set(_lib.exported_symbols()) <= set(_lib._SIGNATURES) | {"maxmulsk_stream_status"}
+
+
+def test_library_is_built_for_sm100a(built_lib):
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", _lib.LIB_PATH],
+                         capture_output=True, text=True).stdout
+    assert "sm_100a" in out
+
+
+def test_status_codes_keep_reference_values(built_lib):
+    # capi/maxmulsk.h:24-28: OK = 0, ERR_UNSUPPORTED = 1, ERR_ALLOC = 2
+    assert (mm.Status.OK, mm.Status.ERR_UNSUPPORTED, mm.Status.ERR_ALLOC) == (0, 1, 2)
+    assert mm.status_string(0) == "MAXMULSK_OK"
+    assert mm.status_string(2) == "MAXMULSK_ERR_ALLOC"
+    assert mm.status_string(5) == "MAXMULSK_ERR_TIMEOUT"
+    assert mm.version() == mm.__version__
+
+
+@pytest.mark.parametrize("plan,ok", [
+    ((0, 128, 128, 1, 0), True), ((0, 128, 64, 4, 1), True), ((0, 64, 64, 64, 0), True),
+    ((0, 64, 128, 1, 0), False), ((0, 128, 128, 0, 0), False), ((0, 128, 128, 65, 0), False),
+    ((0, 128, 128, 1, 2), False), ((1, 128, 256, 1, 0), True), ((2, 128, 64, 8, 0), True),
+    ((3, 128, 128, 1, 0), True), ((1, 64, 128, 1, 0), False), ((1, 128, 96, 1, 0), False),
+    ((1, 128, 128, 1, 1), True), ((1, 128, 128, 1, 2), False), ((4, 128, 128, 1, 0), False), ((-1, 128, 128, 1, 0), False),
+])
+def test_classify(built_lib, plan, ok):
+    p = mm.make_plan(*plan)
+    st = mm.classify(256, 256, 256, p)
+    assert (st == mm.Status.OK) == ok
+    if not ok:
+        assert st == mm.Status.ERR_UNSUPPORTED
+
+
+def test_classify_null_plan(built_lib):
+    assert built_lib.maxmulsk_classify(16, 16, 16, None) == mm.Status.ERR_INVALID
+
+
+def test_workspace_bytes(built_lib):
+    # FP32 without split: no workspace.
+    assert mm.workspace_bytes(512, 512, 512, mm.make_plan(0, 128, 128, 1)) == 0
+    # FP32 with 4 slices: counters + 4 partial C's.
+    M, K, N = 128, 8192, 512
+    ws = mm.workspace_bytes(M, K, N, mm.make_plan(0, 64, 64, 4))
+    assert ws >= 4 * M * N * 4 and ws % 256 == 0
+    # 3xTF32: two FP32 planes of A and of B at least.
+    ws = mm.workspace_bytes(M, K, N, mm.make_plan(1, 128, 128, 1))
+    assert ws >= 2 * 4 * (M * K + K * N)
+    # BF16 x6: three BF16 planes.
+    ws6 = mm.workspace_bytes(M, K, N, mm.make_plan(2, 128, 128, 1))
+    assert 3 * 2 * (M * K + K * N) <= ws6 < ws
+    # invalid plan -> 0
+    assert mm.workspace_bytes(M, K, N, mm.make_plan(0, 32, 32, 1)) == 0
+
+
+def test_slice_rule():
+    assert mm.slice_len(8192, 1) == 8192
+    assert mm.slice_len(8192, 4) == 2048
+    assert mm.slice_len(100, 3) == 64          # rounded up to 32, fewer slices result
+    assert mm.slice_len(20, 8) == 20           # never longer than K
+    for K in (1, 31, 33, 1000, 32768):
+        for s in (1, 2, 3, 7, 64):
+            kc = mm.slice_len(K, s)
+            n = -(-K // kc)
+            assert 1 <= n <= s and (n - 1) * kc < K
+
+
+def test_probe_bytes(built_lib):
+    # As A (R x C = M x K): C padded to 16 bytes, planes 1 KiB aligned.
+    assert built_lib.maxmulsk_probe_split_bytes(4, 5, 1, 0) == 2 * 1024
+    # As B (K x N): N padded to 128 bytes -> 32 floats; 3 planes of BF16 -> 64 bf16 per row.
+    assert built_lib.maxmulsk_probe_split_bytes(1000, 10, 1, 1) == 2 * ((1000 * 32 * 4 + 1023) // 1024 * 1024)
+    assert built_lib.maxmulsk_probe_split_bytes(1000, 10, 2, 1) == 3 * ((1000 * 64 * 2 + 1023) // 1024 * 1024)
+    assert built_lib.maxmulsk_probe_split_bytes(10, 10, 0, 1) == 0

@@ -1,0 +1,132 @@
+"""Split-precision tensor-core path on the GPU against the oracle.
+
+* The split pre-pass planes are compared bit for bit with the oracle's
+  definitions (oracle_split_tf32 / oracle_split_bf16), in the layouts the
+  kernel reads (the counterpart of the reference's pack-layout probes,
+  sme/v4/sme-1x4-kcout-ncblock-apack4za.hpp:44-49, check_nb.cpp:22-39).
+* The tcgen05 GEMM is compared with the oracle's exact split product (the
+  same kept limb pairs, accumulated in FP64): the only difference allowed is
+  the FP32 accumulation, bounded below.
+* Against the FP64 truth, every split mode must stay within 2x the FP32 SIMT
+  kernel's normwise error (plus a floor of 2^-24 for tiny K).
+"""
+import numpy as np
+import pytest
+
+import maxmulsk_b200 as mm
+from gpu_util import bits, run_plan, to_dev
+
+pytestmark = pytest.mark.gpu
+
+MODES = [mm.Precision.TF32X3, mm.Precision.BF16X6, mm.Precision.BF16X9]
+
+
+def _planes_from_probe(cuda, X: np.ndarray, R: int, C: int, prec: int, as_b: bool):
+    nb = mm.lib().maxmulsk_probe_split_bytes(R, C, int(prec), int(as_b))
+    out = cuda.zeros(nb // 4 + 256, dtype=cuda.float32, device="cuda")
+    base = out.data_ptr() + ((-out.data_ptr()) % 1024)
+    dX = to_dev(cuda, X)
+    st = mm.lib().maxmulsk_probe_split_dev(dX.data_ptr(), R, C, int(prec), int(as_b), base, None)
+    assert st == 0
+    cuda.cuda.synchronize()
+    off = (base - out.data_ptr()) // 4
+    return out.cpu().numpy()[off: off + nb // 4].view(np.uint8)[:nb]
+
+
+@pytest.mark.parametrize("prec", [mm.Precision.TF32X3, mm.Precision.BF16X6])
+@pytest.mark.parametrize("as_b", [False, True])
+@pytest.mark.parametrize("shape", [(5, 7), (67, 67), (128, 33), (3, 200)])
+def test_split_planes_bit_exact(cuda, oracle_mod, prec, as_b, shape):
+    R, C = shape
+    X = np.concatenate([oracle_mod.fill_uniform(R * C // 2, 1), oracle_mod.fill_wide(R * C - R * C // 2, 2)])
+    raw = _planes_from_probe(cuda, X, R, C, prec, as_b)
+    tf32 = prec == mm.Precision.TF32X3
+    es = 4 if tf32 else 2
+    P = 2 if tf32 else 3
+    if tf32:
+        want = [p.reshape(R, C) for p in oracle_mod.split_tf32(X)]
+    else:
+        want = [p.reshape(R, C) for p in oracle_mod.split_bf16(X)]
+    Cp = -(-C // (128 // es)) * (128 // es) if as_b else -(-C // (16 // es)) * (16 // es)
+    plane_bytes = -(-(R * Cp * es) // 1024) * 1024
+    for p in range(P):
+        chunk = raw[p * plane_bytes: p * plane_bytes + R * Cp * es]
+        if tf32:
+            v = chunk.view(np.uint32)
+            w = want[p].view(np.uint32)
+        else:
+            v = chunk.view(np.uint16)
+            w = (want[p].view(np.uint32) >> 16).astype(np.uint16)
+        if as_b:
+            nbe = 128 // es
+            v = v.reshape(Cp // nbe, R, nbe).transpose(1, 0, 2).reshape(R, Cp)
+        else:
+            v = v.reshape(R, Cp)
+        assert np.array_equal(v[:, :C], w), p
+        assert np.all(v[:, C:] == 0)
+
+
+SHAPES = [(128, 128, 128), (67, 67, 67), (20, 35, 41), (300, 520, 200), (256, 1024, 512), (1, 64, 1), (130, 16, 300)]
+
+
+@pytest.mark.parametrize("prec", MODES)
+@pytest.mark.parametrize("tile_n", [64, 128, 256])
+@pytest.mark.parametrize("split_k", [1, 3])
+def test_tc_gemm_vs_exact_split_product(cuda, oracle_mod, prec, tile_n, split_k):
+    for i, (M, K, N) in enumerate(SHAPES):
+        A = oracle_mod.fill_uniform(M * K, 30 + i)
+        B = oracle_mod.fill_uniform(K * N, 60 + i)
+        plan = mm.make_plan(prec, 128, tile_n, split_k)
+        st, C, bands = run_plan(cuda, A, B, M, K, N, plan)
+        assert st == 0, mm.last_error_message()
+        assert bands, ((M, K, N), plan)
+        ideal = oracle_mod.sgemm_split_exact(A, B, M, K, N, int(prec))
+        # Only FP32 accumulation separates the two: bounded by K units of
+        # 2^-24 of sum |a||b| <= K for U[-1,1) inputs, far looser in practice.
+        C64 = oracle_mod.dgemm(A, B, M, K, N)
+        e = oracle_mod.errors(C, C64, A, B, M, K, N)
+        e_ideal = oracle_mod.errors(ideal, C64, A, B, M, K, N)
+        assert e["normwise"] <= 4 * e_ideal["normwise"] + 8 * 2.0 ** -24, ((M, K, N), plan, e, e_ideal)
+        assert np.max(np.abs(C - ideal)) <= K * 2.0 ** -22 + 1e-6
+
+
+@pytest.mark.parametrize("kind", ["uniform", "wide"])
+def test_split_error_within_twice_simt(cuda, oracle_mod, kind):
+    M = K = N = 1024
+    fill = oracle_mod.fill_uniform if kind == "uniform" else oracle_mod.fill_wide
+    A, B = fill(M * K, 71), fill(K * N, 72)
+    C64 = oracle_mod.dgemm(A, B, M, K, N)
+    Cs = np.empty(M * N, np.float32)
+    assert mm.sgemm_v3(A, B, Cs, M, K, N) == 0
+    e_simt = oracle_mod.errors(Cs, C64, A, B, M, K, N)
+    for prec in MODES:
+        C = np.empty(M * N, np.float32)
+        assert mm.sgemm_split(A, B, C, M, K, N, prec) == 0, mm.last_error_message()
+        e = oracle_mod.errors(C, C64, A, B, M, K, N)
+        print(kind, int(prec), e, "simt", e_simt)
+        assert e["normwise"] <= 2 * e_simt["normwise"] + 2.0 ** -24, (kind, int(prec), e, e_simt)
+
+
+def test_split_k_deterministic(cuda, oracle_mod):
+    M, K, N = 256, 6000, 384
+    A = oracle_mod.fill_uniform(M * K, 81)
+    B = oracle_mod.fill_uniform(K * N, 82)
+    plan = mm.make_plan(mm.Precision.TF32X3, 128, 128, 8)
+    _, C1, _ = run_plan(cuda, A, B, M, K, N, plan)
+    _, C2, _ = run_plan(cuda, A, B, M, K, N, plan)
+    assert np.array_equal(bits(C1), bits(C2))
+
+
+def test_split_device_entry_and_picker(cuda, oracle_mod):
+    M, K, N = 128, 8192, 512
+    sc = 1.0 / np.sqrt(K)
+    A = oracle_mod.fill_normal(M * K, 91, sc)
+    B = oracle_mod.fill_normal(K * N, 92, sc)
+    dA, dB = to_dev(cuda, A), to_dev(cuda, B)
+    dC = cuda.empty(M * N, device="cuda")
+    assert mm.sgemm_split_dev(dA, dB, dC, M, K, N, mm.Precision.TF32X3) == 0
+    assert mm.stream_status() == 0
+    C = dC.cpu().numpy()
+    C64 = oracle_mod.dgemm(A, B, M, K, N)
+    e = oracle_mod.errors(C, C64, A, B, M, K, N)
+    assert e["rel_frob"] < 1e-5, e
