@@ -155,12 +155,13 @@ maxmulsk_status maxmulsk_sgemm_split_dev(const float* dA, const float* dB, float
 /* TEST ONLY: writes the operand planes the split pre-pass makes from one
  * row-major R x C FP32 matrix, exactly as the tensor-core path does (the
  * analog of NB::probe_pack_A / probe_pack_B,
- * sme/v4/sme-1x4-kcout-ncblock-apack4za.hpp:44-49). as_b == 0 lays planes
- * out as A ([P][R][Cp], Cp = C padded to 16 bytes); as_b != 0 as B
- * ([P][Cp/NBE][R][NBE], Cp = C padded to 128 bytes, NBE = 128 bytes of
- * elements). Planes are FP32 (3xTF32, P = 2) or BF16 (P = 3), each plane
- * starting at a multiple of 1 KiB; out must hold
- * maxmulsk_probe_split_bytes() bytes. Asynchronous on `stream`. */
+ * sme/v4/sme-1x4-kcout-ncblock-apack4za.hpp:44-49). Planes are FP32 (3xTF32,
+ * P = 2) or BF16 (P = 3), each plane starting at a multiple of 1 KiB.
+ *   as_b == 0 (A operand, R x C = M x K): [P][R][Cp], Cp = C padded to 16 bytes.
+ *   as_b != 0 (B operand, R x C = K x N):
+ *     3xTF32: transposed, K-major [P][C][Rp], Rp = R padded to 16 bytes;
+ *     BF16:   N-major panels [P][Cp/NBE][R][NBE], NBE = 64, Cp = C padded to 64.
+ * out must hold maxmulsk_probe_split_bytes() bytes. Asynchronous on `stream`. */
 size_t maxmulsk_probe_split_bytes(size_t R, size_t C, int32_t precision, int32_t as_b);
 maxmulsk_status maxmulsk_probe_split_dev(const float* dX, size_t R, size_t C, int32_t precision,
                                          int32_t as_b, void* out, void* stream);

@@ -56,24 +56,27 @@ struct TcArgs {
     int64_t M, K, N;
     int precision;         // MAXMULSK_PREC_3XTF32 / _BF16X6 / _BF16X9
     int tile_n;            // 64, 128 or 256 (tile_m is 128)
+    int split_k;           // the plan's split_k
     bool reuse_planes;     // skip the split pre-pass: planes are already in place
-    int64_t kchunk;
-    int splits;
     void* planes;          // operand planes written by the split pre-pass
-    float* partial;        // splits * M * N floats when splits > 1
-    unsigned* counters;    // one per output tile when splits > 1
+    float* partial;        // compact partial tiles of the K-split tiles
+    unsigned* counters;    // per split tile and epilogue warp (zero on entry)
     int* err;              // device error word
 };
 size_t tc_workspace_bytes(int64_t M, int64_t K, int64_t N, int precision, int tile_n, int split_k);
+// Bytes of the arrival counters at the start of the partial area (to zero).
+size_t tc_counter_bytes(int64_t M, int64_t K, int64_t N, int tile_n, int split_k);
 bool tc_bind_workspace(TcArgs& a, void* ws, size_t ws_bytes);
 cudaError_t tc_launch(const TcArgs& a, cudaStream_t s);
 
-// Operand plane geometry: A planes are [P][M][Kp] (K-major), B planes are
-// [P][K][Np] (N-major); Kp and Np are padded so rows start on 16-byte (A) and
-// 128-byte (B) boundaries; padding holds zeros.
+// Operand plane geometry. A planes are [P][M][Kp] (K-major). B planes are
+// K-major [P][N][Kp] for TF32, N-major 128-byte panels [P][Np/NBE][K][NBE]
+// for BF16. Kp pads K-major rows to 16 bytes, Np pads N to whole panels;
+// padding holds zeros.
 struct PlaneGeom {
     int P;                 // planes per operand: 2 (TF32) or 3 (BF16)
     int esize;             // bytes per plane element: 4 (TF32) or 2 (BF16)
+    bool b_kmajor;         // B planes K-major (TF32) or N-major panels (BF16)
     int64_t Kp, Np;
     size_t a_plane_bytes, b_plane_bytes;   // one plane, rounded to 1 KiB
 };

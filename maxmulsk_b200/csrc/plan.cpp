@@ -51,6 +51,7 @@ maxmulsk_status classify_plan(size_t M, size_t K, size_t N, const maxmulsk_plan*
             return MAXMULSK_ERR_UNSUPPORTED;
         }
         if (M > kMaxDim || N > kMaxDim || K > kMaxDim) { set_error_message("dimension too large"); return MAXMULSK_ERR_UNSUPPORTED; }
+        if (N > 32ull * 65535ull) { set_error_message("N too large for the split pre-pass grid"); return MAXMULSK_ERR_UNSUPPORTED; }
         return MAXMULSK_OK;
     }
     set_error_message("unknown precision");

@@ -147,16 +147,15 @@ maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t
     a.precision = plan.precision;
     a.tile_n = plan.tile_n;
     a.reuse_planes = (plan.variant == MAXMULSK_TC_REUSE_PLANES);
-    a.kchunk = (int64_t)slice_len(K, plan.split_k);
-    a.splits = slice_count(K, plan.split_k);
+    a.split_k = plan.split_k;
     a.err = ds->err_word;
     if (!tc_bind_workspace(a, ws, ws_bytes)) {
         set_error_message("workspace too small for the tensor-core plan");
         return MAXMULSK_ERR_INVALID;
     }
-    if (a.splits > 1) {
-        const size_t tiles = (size_t)((M + 127) / 128) * ((N + plan.tile_n - 1) / plan.tile_n);
-        st = cuda_status(cudaMemsetAsync(a.counters, 0, tiles * 4 * sizeof(unsigned), s), "cudaMemsetAsync(counters)");
+    if (a.counters) {
+        const size_t cb = tc_counter_bytes((int64_t)M, (int64_t)K, (int64_t)N, plan.tile_n, plan.split_k);
+        st = cuda_status(cudaMemsetAsync(a.counters, 0, cb, s), "cudaMemsetAsync(counters)");
         if (st != MAXMULSK_OK) return st;
     }
     return cuda_status(tc_launch(a, s), "sgemm_split_tc launch");

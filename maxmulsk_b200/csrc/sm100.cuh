@@ -125,6 +125,15 @@ __device__ __forceinline__ void tmem_ld_32x32b_x32(uint32_t taddr, uint32_t (&r)
           "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr) : "memory");
 }
+// 32 lanes x 16 columns.
+__device__ __forceinline__ void tmem_ld_32x32b_x16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr) : "memory");
+}
 __device__ __forceinline__ void tmem_wait_ld() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
@@ -145,13 +154,15 @@ __device__ __forceinline__ uint64_t make_smem_desc(uint32_t saddr, uint32_t lbo_
 }
 
 // Instruction descriptor for kind::tf32 / kind::f16 with FP32 accumulation.
-//   fmt: 1 = BF16, 2 = TF32. A K-major, B MN-major (N contiguous).
-__host__ __device__ constexpr uint32_t make_idesc(uint32_t fmt, uint32_t M, uint32_t N) {
+//   fmt: 1 = BF16, 2 = TF32. A K-major; B K-major (b_mn = 0) or MN-major
+//   (b_mn = 1, N contiguous). Measured on B200: kind::tf32 with an MN-major
+//   B operand yields zeros, so TF32 callers pass b_mn = 0.
+__host__ __device__ constexpr uint32_t make_idesc(uint32_t fmt, uint32_t M, uint32_t N, uint32_t b_mn) {
     return (1u << 4)            // D format F32
          | (fmt << 7)           // A format
          | (fmt << 10)          // B format
          | (0u << 15)           // A K-major
-         | (1u << 16)           // B MN-major
+         | (b_mn << 16)         // B major-ness
          | ((N >> 3) << 17)
          | ((M >> 4) << 24);
 }

@@ -1,12 +1,17 @@
 // Split pre-pass: FP32 operands -> tensor-core operand planes.
 //
 // Replaces the reference's packers (pack_A_streaming / pack_B_streaming,
-// sme/v3/sme-1x4-acc-kcout.cpp:39-193) for the split-precision path. A is
-// written K-major as [P][M][Kp]. B is written N-major in 128-byte column
-// panels, [P][Np/NBE][K][NBE] with NBE = 128 bytes of elements, the GPU
-// counterpart of the reference's 64-column B panels
-// (packed_B[g*K_curr*64 + k*64 + c], :145-193). Padding is zero, so it
-// contributes nothing, like the reference's zero-padded edge packs.
+// sme/v3/sme-1x4-acc-kcout.cpp:39-193) for the split-precision path.
+//   A, every mode : K-major planes [P][M][Kp].
+//   B, 3xTF32     : K-major planes [P][N][Kp] (B transposed on the way: the
+//                   TF32 tensor-core MMA takes B only K-major; with an
+//                   N-major B operand it produces zeros).
+//   B, BF16 modes : N-major planes in 128-byte column panels,
+//                   [P][Np/NBE][K][NBE] with NBE = 64 BF16 elements, the GPU
+//                   counterpart of the reference's 64-column B panels
+//                   (packed_B[g*K_curr*64 + k*64 + c], :145-193).
+// Padding is zero, so it contributes nothing, like the reference's
+// zero-padded edge packs.
 //
 // Planes, from their definitions (finite inputs):
 //   3xTF32 : hi = rna_tf32(x), lo = rna_tf32(x - hi)   (P = 2, stored as FP32
@@ -100,7 +105,44 @@ split_kernel(const float* __restrict__ src, int64_t R, int64_t Cin, int64_t Cout
     }
 }
 
+// B (K x N, row-major) -> TF32 planes of B transposed, [P][N][Kp] with
+// k >= K zero. 32 x 32 tiles through shared memory so that both the read
+// (along n) and the write (along k) are coalesced.
+__global__ void __launch_bounds__(256)
+split_tf32_transpose_kernel(const float* __restrict__ B, int64_t K, int64_t N, int64_t Kp,
+                            float* __restrict__ planes, size_t plane_bytes) {
+    __shared__ float tile[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;     // 32 x 8
+    const int64_t k0 = (int64_t)blockIdx.x * 32, n0 = (int64_t)blockIdx.y * 32;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int64_t k = k0 + ty + 8 * j, n = n0 + tx;
+        tile[ty + 8 * j][tx] = (k < K && n < N) ? __ldcs(B + k * N + n) : 0.0f;
+    }
+    __syncthreads();
+    float* hi_p = planes;
+    float* lo_p = reinterpret_cast<float*>(reinterpret_cast<char*>(planes) + plane_bytes);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int64_t n = n0 + ty + 8 * j, k = k0 + tx;
+        if (n < N && k < Kp) {
+            const float x = tile[tx][ty + 8 * j];
+            const float h = tf32_rna(x);
+            hi_p[n * Kp + k] = h;
+            lo_p[n * Kp + k] = tf32_rna(x - h);
+        }
+    }
+}
+
 inline size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+cudaError_t launch_tf32_transpose(const float* B, int64_t K, int64_t N, int64_t Kp, void* planes,
+                                  size_t plane_bytes, cudaStream_t s) {
+    if (K == 0 || N == 0) return cudaSuccess;
+    dim3 grid((unsigned)((Kp + 31) / 32), (unsigned)((N + 31) / 32));
+    split_tf32_transpose_kernel<<<grid, 256, 0, s>>>(B, K, N, Kp, static_cast<float*>(planes), plane_bytes);
+    return cudaGetLastError();
+}
 
 template <int MODE>
 cudaError_t launch_one(const float* src, int64_t R, int64_t Cin, int64_t Cout, int64_t panel,
@@ -122,12 +164,14 @@ PlaneGeom plane_geom(int64_t M, int64_t K, int64_t N, int precision) {
     const bool tf32 = (precision == MAXMULSK_PREC_3XTF32);
     g.P = tf32 ? 2 : 3;
     g.esize = tf32 ? 4 : 2;
-    // A rows: a multiple of 16 bytes (TMA row stride). B: a whole number of
-    // 128-byte column panels.
+    // K-major rows: a multiple of 16 bytes (TMA row stride). N-major B: a
+    // whole number of 128-byte column panels.
+    g.b_kmajor = tf32;
     g.Kp = (int64_t)round_up((size_t)K, (size_t)(16 / g.esize));
-    g.Np = (int64_t)round_up((size_t)N, (size_t)(128 / g.esize));
+    g.Np = tf32 ? N : (int64_t)round_up((size_t)N, (size_t)(128 / g.esize));
     g.a_plane_bytes = round_up((size_t)M * (size_t)g.Kp * (size_t)g.esize, 1024);
-    g.b_plane_bytes = round_up((size_t)K * (size_t)g.Np * (size_t)g.esize, 1024);
+    g.b_plane_bytes = tf32 ? round_up((size_t)N * (size_t)g.Kp * (size_t)g.esize, 1024)
+                           : round_up((size_t)K * (size_t)g.Np * (size_t)g.esize, 1024);
     return g;
 }
 
@@ -140,7 +184,7 @@ cudaError_t split_launch(const float* A, const float* B, int64_t M, int64_t K, i
     if (precision == MAXMULSK_PREC_3XTF32) {
         e = launch_one<MAXMULSK_PREC_3XTF32>(A, M, K, g.Kp, 0, a_planes, g.a_plane_bytes, s);
         if (e != cudaSuccess) return e;
-        return launch_one<MAXMULSK_PREC_3XTF32>(B, K, N, g.Np, 128 / g.esize, b_planes, g.b_plane_bytes, s);
+        return launch_tf32_transpose(B, K, N, g.Kp, b_planes, g.b_plane_bytes, s);
     }
     e = launch_one<MAXMULSK_PREC_BF16X6>(A, M, K, g.Kp, 0, a_planes, g.a_plane_bytes, s);
     if (e != cudaSuccess) return e;
@@ -156,12 +200,12 @@ size_t split_one_bytes(int64_t R, int64_t C, int precision, bool as_b) {
 cudaError_t split_one(const float* X, int64_t R, int64_t C, int precision, bool as_b, void* out,
                       cudaStream_t s) {
     const PlaneGeom g = as_b ? plane_geom(1, R, C, precision) : plane_geom(R, C, 1, precision);
-    const int64_t cout = as_b ? g.Np : g.Kp;
-    const int64_t panel = as_b ? 128 / g.esize : 0;
-    const size_t pb = as_b ? g.b_plane_bytes : g.a_plane_bytes;
-    if (precision == MAXMULSK_PREC_3XTF32)
-        return launch_one<MAXMULSK_PREC_3XTF32>(X, R, C, cout, panel, out, pb, s);
-    return launch_one<MAXMULSK_PREC_BF16X6>(X, R, C, cout, panel, out, pb, s);
+    if (precision == MAXMULSK_PREC_3XTF32) {
+        if (as_b) return launch_tf32_transpose(X, R, C, g.Kp, out, g.b_plane_bytes, s);
+        return launch_one<MAXMULSK_PREC_3XTF32>(X, R, C, g.Kp, 0, out, g.a_plane_bytes, s);
+    }
+    if (as_b) return launch_one<MAXMULSK_PREC_BF16X6>(X, R, C, g.Np, 128 / g.esize, out, g.b_plane_bytes, s);
+    return launch_one<MAXMULSK_PREC_BF16X6>(X, R, C, g.Kp, 0, out, g.a_plane_bytes, s);
 }
 
 }  // namespace mmsk

@@ -7,22 +7,34 @@
 //   3xTF32 : hi*hi + hi*lo + lo*hi        (tcgen05.mma kind::tf32)
 //   BF16x6 : l_i*l_j for i + j <= 2       (tcgen05.mma kind::f16, BF16)
 //   BF16x9 : all nine l_i*l_j
-// with every product accumulated in one FP32 accumulator in TMEM.
 //
-// Structure (one CTA per SM, persistent; 6 warps):
+// Accuracy. The tensor cores accumulate in FP32 but lose low bits at every
+// accumulation step, so the error of one long TMEM accumulation grows with its
+// length (measured on B200: about 0.4 * L / sqrt(K) times the FP32 SIMT
+// kernel's normwise error for a chain of L k's). The kernel therefore
+// accumulates only KCHUNK = 32 k's in TMEM at a time; the epilogue warps add
+// each chunk into FP32 registers, round to nearest, chunk after chunk in k
+// order. This is the reference's outer-Kc panel scheme (first panel stores,
+// later panels add: sme/v3/sme-1x4-acc-kcout.cpp:464-471, :530-558) with a
+// 32-deep panel, and it keeps the split modes at or below the SIMT kernel's
+// error.
+//
+// Structure (one CTA per SM, persistent):
 //   warp 0      TMA producer: per stage one 3-D load of all A planes
-//               (128 x BK, K-major, 64-byte swizzle) and one 4-D load of all B
-//               planes (BK x BN in 128-byte column panels, 128-byte swizzle),
+//               (128 x BK, K-major, 64-byte swizzle) and one load of all B
+//               planes: K-major BN x BK with 64-byte swizzle (TF32), or
+//               BK x BN in 128-byte column panels with 128-byte swizzle (BF16),
 //               into a ring of STAGES shared-memory stages.
-//   warp 1      TMEM owner; one thread issues the MMAs (128 x BN x KSTEP) and
-//               commits each stage back to the producer.
-//   warps 2..5  epilogue: TMEM -> registers (tcgen05.ld 32x32b) -> global.
-//               Two accumulators in TMEM let the epilogue of one tile overlap
-//               the main loop of the next.
+//   warp 1      TMEM owner; one thread issues the MMAs (128 x BN x KSTEP) of a
+//               chunk into one of two TMEM accumulators and commits each stage
+//               back to the producer and each chunk to the epilogue.
+//   warps 2..   epilogue (4 or 8 warps): TMEM -> registers (tcgen05.ld
+//               32x32b), chunk sums in registers, then global stores. Two TMEM
+//               accumulators let the MMAs of one chunk overlap the drain of
+//               the previous one.
 // Work units are (output tile, K slice) pairs; with several slices per tile,
-// each slice writes a partial and the last slice to arrive (per 32-row
-// quarter) sums the partials in slice order into C, deterministically
-// (the reference's outer-Kc panel order, :464-471 and :530-558).
+// each slice writes a partial and the last slice to arrive (per warp's rows
+// and columns) sums the partials in slice order into C, deterministically.
 //
 // Edges: the TMA boxes read zero outside the planes (M and K tails), the
 // planes are zero-padded in K and N, and the epilogue predicates its stores,
@@ -53,19 +65,25 @@ struct Cfg {
     static constexpr int BK = 64 / ES;              // K per stage: A rows of 64 bytes
     static constexpr int KSTEP = 32 / ES;           // K per MMA (32 bytes)
     static constexpr int KSTEPS = BK / KSTEP;       // 2
-    static constexpr int NBE = 128 / ES;            // N elements per 128-byte panel
-    static constexpr int NBLK = BN / NBE;           // panels per tile
+    static constexpr bool B_KMAJOR = TF32;          // see make_idesc
+    static constexpr int NBE = 128 / ES;            // N elements per 128-byte panel (N-major B)
+    static constexpr int NBLK = BN / NBE;           // panels per tile (N-major B)
     static constexpr int A_PLANE = BM * 64;         // bytes of one A plane per stage
-    static constexpr int B_PLANE = BK * BN * ES;    // bytes of one B plane per stage
+    static constexpr int B_PLANE = BK * BN * ES;    // bytes of one B plane per stage (BN rows of 64 B)
     static constexpr int STAGE = P * (A_PLANE + B_PLANE);
     static constexpr int STAGES_RAW = (220 * 1024) / STAGE;
     static constexpr int STAGES = STAGES_RAW > 8 ? 8 : STAGES_RAW;
     static constexpr int SMEM = STAGES * STAGE + 1024;
     static constexpr int NPROD = TF32 ? 3 : (MODE == MAXMULSK_PREC_BF16X6 ? 6 : 9);
-    static constexpr uint32_t IDESC = make_idesc(TF32 ? 2u : 1u, 128u, (uint32_t)BN);
+    static constexpr uint32_t IDESC = make_idesc(TF32 ? 2u : 1u, 128u, (uint32_t)BN, B_KMAJOR ? 0u : 1u);
     static constexpr uint32_t TMEM_COLS = 2 * BN;
+    // Epilogue: 4 warps (one per TMEM lane quarter) per 128 columns.
+    static constexpr int EPI = (BN >= 256) ? 8 : 4;
+    static constexpr int COLS = BN * 4 / EPI;        // columns per epilogue thread
+    static constexpr int THREADS = 64 + 32 * EPI;
     static_assert(STAGES >= 2, "not enough shared memory for two stages");
-    static_assert(BN % NBE == 0, "tile_n must be a whole number of 128-byte panels");
+    static_assert(COLS % 32 == 0, "column split must be whole");
+    static_assert(B_KMAJOR || BN % NBE == 0, "tile_n must be a whole number of 128-byte panels");
 };
 
 // (A plane, B plane) of each product, in issue order.
@@ -86,23 +104,31 @@ __device__ __forceinline__ void product_planes(int mode, int q, int& pa, int& pb
 
 struct TcParams {
     int64_t M, K, N;
-    int64_t kchunk;
-    int splits;
     int tiles_m, tiles_n;
-    int64_t units;
+    // Schedule: tiles [0, main_tiles) are cut into main_splits K slices of
+    // main_kchunk; tiles [main_tiles, tiles) into tail_splits slices of
+    // tail_kchunk. Units are numbered main region first.
+    int64_t tiles, main_tiles, main_units, units;
+    int main_splits, tail_splits;
+    int64_t main_kchunk, tail_kchunk;
+    int max_splits;
+    int chunk_kb;            // stages per TMEM accumulation chunk
     float* C;
-    float* partial;
-    unsigned* counters;      // 4 per tile (one per 32-row quarter)
+    float* partial;          // [split tile][slice][128 x BN], split tiles only
+    unsigned* counters;      // EPI per split tile (one per epilogue warp)
     int* err;
     long long timeout;       // SM clocks per bounded wait
 };
 
-// Unit -> (tile row, tile column, slice). Slices of one tile are adjacent so
-// they run at the same time; tiles are rastered in groups of 8 tile rows so
+struct Unit {
+    int tm, tn, z, nsplit;
+    int64_t kbeg, kend;
+    int64_t sti;             // index among split tiles, -1 when the tile is whole
+};
+
+// Tile t -> (tile row, tile column), rastered in groups of 8 tile rows so
 // concurrently running CTAs share A rows and B columns in L2.
-__device__ __forceinline__ void decode_unit(const TcParams& p, int64_t u, int& tm, int& tn, int& z) {
-    z = (int)(u % p.splits);
-    const int64_t t = u / p.splits;
+__device__ __forceinline__ void tile_coords(const TcParams& p, int64_t t, int& tm, int& tn) {
     constexpr int G = 8;
     const int64_t per_group = (int64_t)G * p.tiles_n;
     const int64_t g = t / per_group;
@@ -113,11 +139,38 @@ __device__ __forceinline__ void decode_unit(const TcParams& p, int64_t u, int& t
     tn = (int)(r / gsz);
 }
 
+// Unit -> its tile, K slice and where its partial goes. Slices of one tile
+// are adjacent so they run at the same time.
+__device__ __forceinline__ Unit decode_unit(const TcParams& p, int64_t u) {
+    Unit w;
+    int64_t t;
+    int64_t kc;
+    if (u < p.main_units) {
+        w.z = (int)(u % p.main_splits);
+        t = u / p.main_splits;
+        w.nsplit = p.main_splits;
+        kc = p.main_kchunk;
+        w.sti = (p.main_splits > 1) ? t : -1;
+    } else {
+        const int64_t v = u - p.main_units;
+        w.z = (int)(v % p.tail_splits);
+        t = p.main_tiles + v / p.tail_splits;
+        w.nsplit = p.tail_splits;
+        kc = p.tail_kchunk;
+        w.sti = (p.tail_splits > 1) ? t - p.main_tiles : -1;
+    }
+    w.kbeg = (int64_t)w.z * kc;
+    w.kend = min(p.K, w.kbeg + kc);
+    tile_coords(p, t, w.tm, w.tn);
+    return w;
+}
+
 template <int MODE, int BN>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(Cfg<MODE, BN>::THREADS, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                const TcParams p) {
     using Cf = Cfg<MODE, BN>;
+    constexpr int COLS = Cf::COLS;                   // columns of one epilogue thread
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[Cf::STAGES];
     __shared__ __align__(8) uint64_t empty_bar[Cf::STAGES];
@@ -133,7 +186,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < Cf::STAGES; s++) { mbar_init(&full_bar[s], 1); mbar_init(&empty_bar[s], 1); }
-        for (int a = 0; a < 2; a++) { mbar_init(&tfull_bar[a], 1); mbar_init(&tempty_bar[a], 4); }
+        for (int a = 0; a < 2; a++) { mbar_init(&tfull_bar[a], 1); mbar_init(&tempty_bar[a], Cf::EPI); }
         mbar_init(&done_bar, 1);
         abort_s = 0;
         fence_mbar_init();
@@ -150,6 +203,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         atomicOr(p.err, kErrTimeout);
         abort_s = 1;
     };
+    auto kblocks = [&](const Unit& w) -> int64_t { return (w.kend - w.kbeg + Cf::BK - 1) / Cf::BK; };
 
     if (warp == 0) {
         // ------------------------------------------------------------ producer
@@ -158,11 +212,8 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             uint32_t phase = 0;
             int64_t issued = 0;
             for (int64_t u = blockIdx.x; u < p.units && !abort_s; u += gridDim.x) {
-                int tm, tn, z;
-                decode_unit(p, u, tm, tn, z);
-                const int64_t kbeg = (int64_t)z * p.kchunk;
-                const int64_t kend = min(p.K, kbeg + p.kchunk);
-                const int64_t nkb = (kend - kbeg + Cf::BK - 1) / Cf::BK;
+                const Unit w = decode_unit(p, u);
+                const int64_t nkb = kblocks(w);
                 bool ok = true;
                 for (int64_t kb = 0; kb < nkb; kb++) {
                     if (!mbar_wait_bounded(&empty_bar[stage], phase ^ 1u, p.timeout)) { fail(); ok = false; break; }
@@ -170,9 +221,10 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                     uint8_t* sa = smem + (size_t)stage * Cf::STAGE;
                     uint8_t* sb = sa + Cf::P * Cf::A_PLANE;
                     mbar_arrive_expect_tx(&full_bar[stage], (uint32_t)Cf::STAGE);
-                    const int32_t k = (int32_t)(kbeg + kb * Cf::BK);
-                    tma_load_3d(sa, &tmA, &full_bar[stage], k, tm * Cf::BM, 0);
-                    tma_load_4d(sb, &tmB, &full_bar[stage], 0, k, tn * Cf::NBLK, 0);
+                    const int32_t k = (int32_t)(w.kbeg + kb * Cf::BK);
+                    tma_load_3d(sa, &tmA, &full_bar[stage], k, w.tm * Cf::BM, 0);
+                    if constexpr (Cf::B_KMAJOR) tma_load_3d(sb, &tmB, &full_bar[stage], k, w.tn * BN, 0);
+                    else tma_load_4d(sb, &tmB, &full_bar[stage], 0, k, w.tn * Cf::NBLK, 0);
                     issued++;
                     if (++stage == Cf::STAGES) { stage = 0; phase ^= 1u; }
                 }
@@ -194,43 +246,44 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             uint32_t phase = 0;
             int acc = 0;
             uint32_t acc_phase = 0;
-            for (int64_t u = blockIdx.x; u < p.units && !abort_s; u += gridDim.x) {
-                int tm, tn, z;
-                decode_unit(p, u, tm, tn, z);
-                const int64_t kbeg = (int64_t)z * p.kchunk;
-                const int64_t kend = min(p.K, kbeg + p.kchunk);
-                const int64_t nkb = (kend - kbeg + Cf::BK - 1) / Cf::BK;
-                if (!mbar_wait_bounded(&tempty_bar[acc], acc_phase ^ 1u, p.timeout)) { fail(); break; }
-                tc_fence_after();
-                const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
-                bool ok = true;
-                for (int64_t kb = 0; kb < nkb; kb++) {
-                    if (!mbar_wait_bounded(&full_bar[stage], phase, p.timeout)) { fail(); ok = false; break; }
+            bool ok = true;
+            for (int64_t u = blockIdx.x; u < p.units && ok && !abort_s; u += gridDim.x) {
+                const int64_t nkb = kblocks(decode_unit(p, u));
+                for (int64_t kb0 = 0; kb0 < nkb && ok; kb0 += p.chunk_kb) {
+                    // one chunk of up to CHUNK_KB stages into accumulator `acc`
+                    if (!mbar_wait_bounded(&tempty_bar[acc], acc_phase ^ 1u, p.timeout)) { fail(); ok = false; break; }
                     tc_fence_after();
-                    const uint32_t a_base = smem_u32(smem + (size_t)stage * Cf::STAGE);
-                    const uint32_t b_base = a_base + Cf::P * Cf::A_PLANE;
+                    const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+                    const int64_t kb1 = min(nkb, kb0 + (int64_t)p.chunk_kb);
+                    for (int64_t kb = kb0; kb < kb1; kb++) {
+                        if (!mbar_wait_bounded(&full_bar[stage], phase, p.timeout)) { fail(); ok = false; break; }
+                        tc_fence_after();
+                        const uint32_t a_base = smem_u32(smem + (size_t)stage * Cf::STAGE);
+                        const uint32_t b_base = a_base + Cf::P * Cf::A_PLANE;
 #pragma unroll
-                    for (int ks = 0; ks < Cf::KSTEPS; ks++) {
+                        for (int ks = 0; ks < Cf::KSTEPS; ks++) {
 #pragma unroll
-                        for (int q = 0; q < Cf::NPROD; q++) {
-                            int pa, pb;
-                            product_planes(MODE, q, pa, pb);
-                            const uint64_t adesc = make_smem_desc(
-                                a_base + (uint32_t)(pa * Cf::A_PLANE + ks * 32), 16u, 512u, 4u);
-                            const uint64_t bdesc = make_smem_desc(
-                                b_base + (uint32_t)(pb * Cf::B_PLANE + ks * Cf::KSTEP * 128),
-                                (uint32_t)(Cf::BK * 128), 1024u, 2u);
-                            const uint32_t accum = (kb > 0 || ks > 0 || q > 0) ? 1u : 0u;
-                            if constexpr (Cf::TF32) mma_tf32(d_tmem, adesc, bdesc, Cf::IDESC, accum);
-                            else mma_bf16(d_tmem, adesc, bdesc, Cf::IDESC, accum);
+                            for (int q = 0; q < Cf::NPROD; q++) {
+                                int pa, pb;
+                                product_planes(MODE, q, pa, pb);
+                                const uint64_t adesc = make_smem_desc(
+                                    a_base + (uint32_t)(pa * Cf::A_PLANE + ks * 32), 16u, 512u, 4u);
+                                const uint64_t bdesc = Cf::B_KMAJOR
+                                    ? make_smem_desc(b_base + (uint32_t)(pb * Cf::B_PLANE + ks * 32), 16u, 512u, 4u)
+                                    : make_smem_desc(b_base + (uint32_t)(pb * Cf::B_PLANE + ks * Cf::KSTEP * 128),
+                                                     (uint32_t)(Cf::BK * 128), 1024u, 2u);
+                                const uint32_t accum = (kb > kb0 || ks > 0 || q > 0) ? 1u : 0u;
+                                if constexpr (Cf::TF32) mma_tf32(d_tmem, adesc, bdesc, Cf::IDESC, accum);
+                                else mma_bf16(d_tmem, adesc, bdesc, Cf::IDESC, accum);
+                            }
                         }
+                        tc_commit(&empty_bar[stage]);
+                        if (++stage == Cf::STAGES) { stage = 0; phase ^= 1u; }
                     }
-                    tc_commit(&empty_bar[stage]);
-                    if (++stage == Cf::STAGES) { stage = 0; phase ^= 1u; }
+                    if (!ok) break;
+                    tc_commit(&tfull_bar[acc]);
+                    if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
                 }
-                if (!ok) break;
-                tc_commit(&tfull_bar[acc]);
-                if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
             }
             // No MMA may still be running when TMEM is freed.
             tc_commit(&done_bar);
@@ -238,80 +291,99 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
     } else {
         // ------------------------------------------------------------ epilogue
+        const int ew = warp - 2;                      // epilogue warp 0 .. EPI-1
         const int quarter = warp & 3;                 // TMEM lanes 32*quarter .. +31
+        const int cgroup = ew / 4;                    // which COLS-wide column group
         const int64_t M = p.M, N = p.N;
-        const size_t MN = (size_t)M * (size_t)N;
         const bool vec = (N % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) &&
                          (p.partial == nullptr || (reinterpret_cast<uintptr_t>(p.partial) & 15) == 0);
         int acc = 0;
         uint32_t acc_phase = 0;
-        for (int64_t u = blockIdx.x; u < p.units; u += gridDim.x) {
-            int stop = abort_s;
-            int tm, tn, z;
-            decode_unit(p, u, tm, tn, z);
-            if (!stop && lane == 0) {
-                if (!mbar_wait_bounded(&tfull_bar[acc], acc_phase, p.timeout)) { fail(); stop = 1; }
-            }
-            stop = __shfl_sync(0xffffffffu, stop, 0);
-            if (stop) break;
-            __syncwarp();
-            tc_fence_after();
-            const int64_t row = (int64_t)tm * Cf::BM + quarter * 32 + lane;
-            const int64_t col0 = (int64_t)tn * BN;
-            float* out = (p.splits > 1) ? p.partial + (size_t)z * MN : p.C;
-#pragma unroll 1
-            for (int c = 0; c < BN; c += 32) {
-                uint32_t r[32];
-                tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + c), r);
-                tmem_wait_ld();
-                if (row < M) {
-                    const int64_t cb = col0 + c;
-                    float* dst = out + (size_t)row * (size_t)N + (size_t)cb;
-                    if (vec && cb + 31 < N) {
+        float sum[COLS];
+        bool stop = false;
+        for (int64_t u = blockIdx.x; u < p.units && !stop; u += gridDim.x) {
+            const Unit w = decode_unit(p, u);
+            const int64_t nkb = kblocks(w);
+            for (int64_t kb0 = 0; kb0 < nkb; kb0 += p.chunk_kb) {
+                int bad = abort_s;
+                if (!bad && lane == 0) {
+                    if (!mbar_wait_bounded(&tfull_bar[acc], acc_phase, p.timeout)) { fail(); bad = 1; }
+                }
+                bad = __shfl_sync(0xffffffffu, bad, 0);
+                if (bad) { stop = true; break; }
+                tc_fence_after();
+                const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + cgroup * COLS);
 #pragma unroll
-                        for (int j = 0; j < 32; j += 4)
-                            *reinterpret_cast<float4*>(dst + j) =
-                                make_float4(__uint_as_float(r[j]), __uint_as_float(r[j + 1]),
-                                            __uint_as_float(r[j + 2]), __uint_as_float(r[j + 3]));
+                for (int c = 0; c < COLS; c += 16) {
+                    uint32_t r[16];
+                    tmem_ld_32x32b_x16(taddr + (uint32_t)c, r);
+                    tmem_wait_ld();
+                    if (kb0 == 0) {
+#pragma unroll
+                        for (int j = 0; j < 16; j++) sum[c + j] = __uint_as_float(r[j]);
                     } else {
 #pragma unroll
-                        for (int j = 0; j < 32; j++)
-                            if (cb + j < N) dst[j] = __uint_as_float(r[j]);
+                        for (int j = 0; j < 16; j++) sum[c + j] = __fadd_rn(sum[c + j], __uint_as_float(r[j]));
                     }
                 }
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&tempty_bar[acc]);
-            if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
-
-            if (p.splits > 1) {
-                // This quarter's partial is written; the last slice to arrive
-                // sums all slices in slice order.
-                __threadfence();
+                tc_fence_before();
                 __syncwarp();
-                int last = 0;
-                const int64_t tile = (int64_t)tm * p.tiles_n + tn;
-                unsigned* ctr = p.counters + tile * 4 + quarter;
-                if (lane == 0) last = (atomicAdd(ctr, 1u) == (unsigned)(p.splits - 1));
-                last = __shfl_sync(0xffffffffu, last, 0);
-                if (last) {
-                    __threadfence();
-                    const int64_t r0 = (int64_t)tm * Cf::BM + quarter * 32;
-                    for (int rr = 0; rr < 32; rr++) {
-                        const int64_t rw = r0 + rr;
-                        if (rw >= M) break;
-                        for (int c = lane; c < BN; c += 32) {
-                            const int64_t cc = col0 + c;
-                            if (cc >= N) break;
-                            const size_t off = (size_t)rw * (size_t)N + (size_t)cc;
-                            float s = __ldcg(p.partial + off);
-                            for (int q = 1; q < p.splits; q++) s = __fadd_rn(s, __ldcg(p.partial + (size_t)q * MN + off));
-                            p.C[off] = s;
-                        }
+                if (lane == 0) mbar_arrive(&tempty_bar[acc]);
+                if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+            }
+            if (stop) break;
+
+            // ---- the unit's sums are complete: store them
+            const int lrow = quarter * 32 + lane;             // row within the tile
+            const int lcol = cgroup * COLS;                   // first column within the tile
+            const int64_t row = (int64_t)w.tm * Cf::BM + lrow;
+            const int64_t col0 = (int64_t)w.tn * BN + lcol;
+            if (w.sti < 0) {
+                if (row < M) {
+                    float* dst = p.C + (size_t)row * (size_t)N + (size_t)col0;
+                    if (vec && col0 + COLS <= N) {
+#pragma unroll
+                        for (int j = 0; j < COLS; j += 4)
+                            *reinterpret_cast<float4*>(dst + j) = make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < COLS; j++)
+                            if (col0 + j < N) dst[j] = sum[j];
                     }
-                    if (lane == 0) *ctr = 0u;
                 }
+                continue;
+            }
+            // A slice of a split tile: write the partial tile (compact, whole
+            // rows), then the last slice to arrive for this warp's rows and
+            // columns sums all slices in slice order into C.
+            constexpr size_t TILE = (size_t)Cf::BM * BN;
+            float* part = p.partial + ((size_t)w.sti * p.max_splits + w.z) * TILE + (size_t)lrow * BN + lcol;
+#pragma unroll
+            for (int j = 0; j < COLS; j += 4)
+                __stcg(reinterpret_cast<float4*>(part + j), make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]));
+            __threadfence();
+            __syncwarp();
+            int last = 0;
+            unsigned* ctr = p.counters + (size_t)w.sti * Cf::EPI + ew;
+            if (lane == 0) last = (atomicAdd(ctr, 1u) == (unsigned)(w.nsplit - 1));
+            last = __shfl_sync(0xffffffffu, last, 0);
+            if (last) {
+                __threadfence();
+                const float* base = p.partial + (size_t)w.sti * p.max_splits * TILE;
+                for (int rr = 0; rr < 32; rr++) {
+                    const int lr = quarter * 32 + rr;
+                    const int64_t grow = (int64_t)w.tm * Cf::BM + lr;
+                    if (grow >= M) break;
+                    for (int c = lane; c < COLS; c += 32) {
+                        const int64_t gcol = col0 + c;
+                        if (gcol >= N) break;
+                        const size_t off = (size_t)lr * BN + lcol + c;
+                        float v = __ldcg(base + off);
+                        for (int q = 1; q < w.nsplit; q++) v = __fadd_rn(v, __ldcg(base + (size_t)q * TILE + off));
+                        p.C[(size_t)grow * (size_t)N + (size_t)gcol] = v;
+                    }
+                }
+                if (lane == 0) *ctr = 0u;
             }
         }
     }
@@ -344,8 +416,68 @@ EncodeTiledFn get_encode_fn() {
 
 inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
-size_t tiles_of(int64_t M, int64_t N, int tile_n) {
-    return (size_t)((M + 127) / 128) * (size_t)((N + tile_n - 1) / tile_n);
+// Host-side schedule of one launch (see TcParams).
+struct Sched {
+    int64_t tiles_m, tiles_n, tiles;
+    int64_t main_tiles, main_units, units;
+    int main_splits, tail_splits;
+    int64_t main_kchunk, tail_kchunk;
+    int64_t split_tiles;
+    int max_splits;
+    int64_t grid;
+};
+
+// With no K split requested and a last wave that would leave SMs idle
+// (tiles = w * SMs + r, 0 < r <= SMs / 2), the r tiles of that wave are cut
+// into floor(SMs / r) K slices so the wave is shared by all SMs.
+Sched make_sched(int64_t M, int64_t K, int64_t N, int tile_n, int split_k, int sms) {
+    Sched s{};
+    s.tiles_m = (M + 127) / 128;
+    s.tiles_n = (N + tile_n - 1) / tile_n;
+    s.tiles = s.tiles_m * s.tiles_n;
+    s.main_splits = slice_count((size_t)K, split_k);
+    s.main_kchunk = (int64_t)slice_len((size_t)K, split_k);
+    s.main_tiles = s.tiles;
+    s.tail_splits = 1;
+    s.tail_kchunk = K;
+    if (sms <= 0) sms = 148;
+    if (s.main_splits == 1 && s.tiles > sms) {
+        const int64_t r = s.tiles % sms;
+        if (r > 0 && r <= sms / 2) {
+            int want = (int)(sms / r);
+            const int64_t max_by_k = K / 256;          // keep slices at least 256 deep
+            if (want > max_by_k) want = (int)max_by_k;
+            if (want > 1) {
+                const int tail = slice_count((size_t)K, want);
+                if (tail > 1) {
+                    s.tail_splits = tail;
+                    s.tail_kchunk = (int64_t)slice_len((size_t)K, want);
+                    s.main_tiles = s.tiles - r;
+                }
+            }
+        }
+    }
+    s.main_units = s.main_tiles * s.main_splits;
+    s.units = s.main_units + (s.tiles - s.main_tiles) * s.tail_splits;
+    if (s.main_splits > 1) { s.split_tiles = s.tiles; s.max_splits = s.main_splits; }
+    else if (s.tail_splits > 1) { s.split_tiles = s.tiles - s.main_tiles; s.max_splits = s.tail_splits; }
+    else { s.split_tiles = 0; s.max_splits = 1; }
+    s.grid = s.units < sms ? s.units : sms;
+    return s;
+}
+
+// K per TMEM accumulation chunk: 32, 64 or 128 as K grows, which keeps the
+// accumulation error near a constant fraction of the FP32 SIMT kernel's.
+int chunk_len(int64_t K) {
+    if (K >= 16384) return 128;
+    if (K >= 4096) return 64;
+    return 32;
+}
+
+size_t partial_bytes(const Sched& s, int tile_n) {
+    if (s.split_tiles == 0) return 0;
+    return align256((size_t)s.split_tiles * 8 * sizeof(unsigned)) +
+           align256((size_t)s.split_tiles * s.max_splits * 128 * (size_t)tile_n * sizeof(float));
 }
 
 template <int MODE, int BN>
@@ -369,7 +501,16 @@ cudaError_t launch_cfg(const TcArgs& a, cudaStream_t s) {
                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
             return cudaErrorInvalidValue;
     }
-    {
+    if constexpr (Cf::B_KMAJOR) {
+        const cuuint64_t dims[3] = {(cuuint64_t)g.Kp, (cuuint64_t)a.N, (cuuint64_t)g.P};
+        const cuuint64_t strides[2] = {(cuuint64_t)g.Kp * Cf::ES, (cuuint64_t)g.b_plane_bytes};
+        const cuuint32_t box[3] = {(cuuint32_t)Cf::BK, (cuuint32_t)BN, (cuuint32_t)Cf::P};
+        const cuuint32_t estr[3] = {1, 1, 1};
+        if (enc(&tmB, dt, 3, b_planes, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return cudaErrorInvalidValue;
+    } else {
         const cuuint64_t npan = (cuuint64_t)(g.Np / Cf::NBE);
         const cuuint64_t dims[4] = {(cuuint64_t)Cf::NBE, (cuuint64_t)a.K, npan, (cuuint64_t)g.P};
         const cuuint64_t strides[3] = {128u, (cuuint64_t)a.K * 128u, (cuuint64_t)g.b_plane_bytes};
@@ -381,26 +522,33 @@ cudaError_t launch_cfg(const TcArgs& a, cudaStream_t s) {
             return cudaErrorInvalidValue;
     }
 
+    const Sched sc = make_sched(a.M, a.K, a.N, BN, a.split_k, device_sm_count());
     TcParams prm;
     prm.M = a.M; prm.K = a.K; prm.N = a.N;
-    prm.kchunk = a.kchunk;
-    prm.splits = a.splits;
-    prm.tiles_m = (int)((a.M + 127) / 128);
-    prm.tiles_n = (int)((a.N + BN - 1) / BN);
-    prm.units = (int64_t)prm.tiles_m * prm.tiles_n * a.splits;
+    prm.tiles_m = (int)sc.tiles_m;
+    prm.tiles_n = (int)sc.tiles_n;
+    prm.tiles = sc.tiles;
+    prm.main_tiles = sc.main_tiles;
+    prm.main_units = sc.main_units;
+    prm.units = sc.units;
+    prm.main_splits = sc.main_splits;
+    prm.tail_splits = sc.tail_splits;
+    prm.main_kchunk = sc.main_kchunk;
+    prm.tail_kchunk = sc.tail_kchunk;
+    prm.max_splits = sc.max_splits;
+    prm.chunk_kb = chunk_len(a.K) / Cf::BK;
     prm.C = a.C;
     prm.partial = a.partial;
     prm.counters = a.counters;
     prm.err = a.err;
     prm.timeout = 2000000000LL;   // about one second at B200 clocks
+    if (sc.split_tiles > 0 && (!a.partial || !a.counters)) return cudaErrorInvalidValue;
 
     // Per device and cheap; set on every launch so every device gets it.
     cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<MODE, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          Cf::SMEM);
     if (e != cudaSuccess) return e;
-    const int sms = device_sm_count();
-    const int64_t grid = prm.units < sms ? prm.units : sms;
-    tc_gemm_kernel<MODE, BN><<<(unsigned)grid, 192, Cf::SMEM, s>>>(tmA, tmB, prm);
+    tc_gemm_kernel<MODE, BN><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, prm);
     return cudaGetLastError();
 }
 
@@ -418,30 +566,26 @@ cudaError_t launch_mode(const TcArgs& a, cudaStream_t s) {
 
 size_t tc_workspace_bytes(int64_t M, int64_t K, int64_t N, int precision, int tile_n, int split_k) {
     const PlaneGeom g = plane_geom(M, K, N, precision);
-    size_t bytes = (size_t)g.P * (g.a_plane_bytes + g.b_plane_bytes);
-    const int splits = slice_count((size_t)K, split_k);
-    if (splits > 1) {
-        bytes += align256(tiles_of(M, N, tile_n) * 4 * sizeof(unsigned));
-        bytes += align256((size_t)splits * (size_t)M * (size_t)N * sizeof(float));
-    }
-    return align256(bytes);
+    const Sched sc = make_sched(M, K, N, tile_n, split_k, device_sm_count());
+    return align256((size_t)g.P * (g.a_plane_bytes + g.b_plane_bytes)) + partial_bytes(sc, tile_n);
+}
+
+size_t tc_counter_bytes(int64_t M, int64_t K, int64_t N, int tile_n, int split_k) {
+    const Sched sc = make_sched(M, K, N, tile_n, split_k, device_sm_count());
+    return (size_t)sc.split_tiles * 8 * sizeof(unsigned);
 }
 
 bool tc_bind_workspace(TcArgs& a, void* ws, size_t ws_bytes) {
     const PlaneGeom g = plane_geom(a.M, a.K, a.N, a.precision);
-    size_t need = (size_t)g.P * (g.a_plane_bytes + g.b_plane_bytes);
-    if (a.splits > 1) {
-        need += align256(tiles_of(a.M, a.N, a.tile_n) * 4 * sizeof(unsigned));
-        need += align256((size_t)a.splits * (size_t)a.M * (size_t)a.N * sizeof(float));
-    }
+    const Sched sc = make_sched(a.M, a.K, a.N, a.tile_n, a.split_k, device_sm_count());
+    const size_t planes = align256((size_t)g.P * (g.a_plane_bytes + g.b_plane_bytes));
+    const size_t need = planes + partial_bytes(sc, a.tile_n);
     if (!ws || ws_bytes < need || (reinterpret_cast<uintptr_t>(ws) & 255) != 0) return false;
     char* base = static_cast<char*>(ws);
     a.planes = base;
-    base += (size_t)g.P * (g.a_plane_bytes + g.b_plane_bytes);
-    if (a.splits > 1) {
-        a.counters = reinterpret_cast<unsigned*>(base);
-        base += align256(tiles_of(a.M, a.N, a.tile_n) * 4 * sizeof(unsigned));
-        a.partial = reinterpret_cast<float*>(base);
+    if (sc.split_tiles > 0) {
+        a.counters = reinterpret_cast<unsigned*>(base + planes);
+        a.partial = reinterpret_cast<float*>(base + planes + align256((size_t)sc.split_tiles * 8 * sizeof(unsigned)));
     } else {
         a.counters = nullptr;
         a.partial = nullptr;

@@ -90,7 +90,8 @@ def test_slice_rule():
 def test_probe_bytes(built_lib):
     # As A (R x C = M x K): C padded to 16 bytes, planes 1 KiB aligned.
     assert built_lib.maxmulsk_probe_split_bytes(4, 5, 1, 0) == 2 * 1024
-    # As B (K x N): N padded to 128 bytes -> 32 floats; 3 planes of BF16 -> 64 bf16 per row.
-    assert built_lib.maxmulsk_probe_split_bytes(1000, 10, 1, 1) == 2 * ((1000 * 32 * 4 + 1023) // 1024 * 1024)
+    # As B (K x N), TF32: transposed N x Kp, Kp = K padded to 4 floats.
+    assert built_lib.maxmulsk_probe_split_bytes(1000, 10, 1, 1) == 2 * ((10 * 1000 * 4 + 1023) // 1024 * 1024)
+    # As B, BF16: N padded to 64 elements (128 bytes), 3 planes.
     assert built_lib.maxmulsk_probe_split_bytes(1000, 10, 2, 1) == 3 * ((1000 * 64 * 2 + 1023) // 1024 * 1024)
     assert built_lib.maxmulsk_probe_split_bytes(10, 10, 0, 1) == 0

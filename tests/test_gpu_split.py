@@ -47,16 +47,25 @@ def test_split_planes_bit_exact(cuda, oracle_mod, prec, as_b, shape):
         want = [p.reshape(R, C) for p in oracle_mod.split_tf32(X)]
     else:
         want = [p.reshape(R, C) for p in oracle_mod.split_bf16(X)]
-    Cp = -(-C // (128 // es)) * (128 // es) if as_b else -(-C // (16 // es)) * (16 // es)
-    plane_bytes = -(-(R * Cp * es) // 1024) * 1024
+    if as_b and tf32:
+        # transposed: [P][C][Rp], K-major
+        Rp = -(-R // 4) * 4
+        plane_bytes = -(-(C * Rp * es) // 1024) * 1024
+    else:
+        Cp = -(-C // (128 // es)) * (128 // es) if as_b else -(-C // (16 // es)) * (16 // es)
+        plane_bytes = -(-(R * Cp * es) // 1024) * 1024
     for p in range(P):
-        chunk = raw[p * plane_bytes: p * plane_bytes + R * Cp * es]
         if tf32:
-            v = chunk.view(np.uint32)
             w = want[p].view(np.uint32)
         else:
-            v = chunk.view(np.uint16)
             w = (want[p].view(np.uint32) >> 16).astype(np.uint16)
+        if as_b and tf32:
+            v = raw[p * plane_bytes: p * plane_bytes + C * Rp * es].view(np.uint32).reshape(C, Rp)
+            assert np.array_equal(v[:, :R].T, w), p
+            assert np.all(v[:, R:] == 0)
+            continue
+        chunk = raw[p * plane_bytes: p * plane_bytes + R * Cp * es]
+        v = chunk.view(np.uint32) if tf32 else chunk.view(np.uint16)
         if as_b:
             nbe = 128 // es
             v = v.reshape(Cp // nbe, R, nbe).transpose(1, 0, 2).reshape(R, Cp)
