@@ -222,7 +222,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--size", type=int, default=4096)
-    ap.add_argument("--precision", choices=list(PREC), default="tf32x3")
+    ap.add_argument("--precision", choices=list(PREC), default="bf16x6")
     ap.add_argument("--no-extras", action="store_true", help="headline timing only (for profiling runs)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -370,6 +370,24 @@ def main() -> None:
                        "plan": {"tile_m": splan.tile_m, "tile_n": splan.tile_n, "split_k": splan.split_k},
                        "peak_tflops": fp32_peak_max, "frac": simt_gf / 1e3 / fp32_peak_max,
                        "peak_basis": "nominal FP32 FMA: 148 SMs x 128 lanes x 2 x max SM clock"}
+        # ---- the other split modes, same inputs (pre-pass + GEMM per step)
+        modes = {}
+        for name, pc in PREC.items():
+            mp = mm.choose(M, K, N, pc)
+            mb = mm.workspace_bytes(M, K, N, mp)
+            mws = torch.empty(mb + 256, dtype=torch.uint8, device=dev)
+            mwp = mws.data_ptr() + ((-mws.data_ptr()) % 256)
+            dCm = torch.empty((M, N), dtype=torch.float32, device=dev)
+
+            def step_mode(mp=mp, mwp=mwp, mb=mb, dCm=dCm):
+                mm.check(mm.sgemm_plan_dev(dA, dB, dCm, M, K, N, mp, mwp, mb, stream), "mode step")
+            for _ in range(3):
+                step_mode()
+            t_m = timed(step_mode, max(10, min(args.steps, 50)))
+            modes[name] = {"gflops": flops / t_m / 1e9, "ms_per_step": t_m * 1e3,
+                           "plan": {"tile_m": mp.tile_m, "tile_n": mp.tile_n, "split_k": mp.split_k},
+                           "_C": dCm}
+            del mws
         out["speedup_vs_simt"] = (flops / t_step) / (flops / t_simt)
         out["speedup_vs_simt_gemm_only"] = t_simt / t_gemm
         out["gpu_launches"] = 3 * args.steps
@@ -381,13 +399,19 @@ def main() -> None:
                 floor = (A64.abs() @ B64.abs()) * 2.0 ** -24
                 nab = torch.linalg.norm(A64) * torch.linalg.norm(B64)
                 errs = {}
-                for name, Cx in (("tc", dC), ("simt", dCs)):
+                for name, Cx in [("tc", dC), ("simt", dCs)] + [(k, v["_C"]) for k, v in modes.items()]:
                     d = (Cx.double() - C64).abs()
                     errs[name] = {"normwise": float(torch.linalg.norm(d) / nab),
                                   "max_rel": float((d / torch.maximum(C64.abs(), floor)).max())}
                 del A64, B64, C64, floor
             errs["tc_over_simt_normwise"] = errs["tc"]["normwise"] / errs["simt"]["normwise"]
-            out["fp64_error"] = errs
+            out["fp64_error"] = {"tc": errs["tc"], "simt": errs["simt"],
+                                 "tc_over_simt_normwise": errs["tc_over_simt_normwise"]}
+            for k in modes:
+                modes[k]["normwise_over_simt"] = errs[k]["normwise"] / errs["simt"]["normwise"]
+        for k in modes:
+            modes[k].pop("_C", None)
+        out["split_modes"] = modes
         # ---- end to end through the public host-pointer API (pinned host buffers)
         hA = torch.from_numpy(A).pin_memory()
         hB = torch.from_numpy(B).pin_memory()

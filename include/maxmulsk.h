@@ -94,8 +94,9 @@ enum {
 /* The analog of the reference's Blocking (sme/v4/sme-1x4-kcout-ncblock-apack4za.hpp:30,
  * sme/support/gemm_tuning.hpp:37-43): how one GEMM is cut into work.
  *   precision : maxmulsk_precision
- *   tile_m, tile_n : output tile of one CTA. FP32: 128x128, 128x64, 64x64.
- *                    Tensor cores: tile_m 128, tile_n 64, 128 or 256.
+ *   tile_m, tile_n : output tile. FP32 (one CTA): 128x128, 128x64, 64x64.
+ *                    Tensor cores: 128 x {64, 128, 256} on one CTA, or
+ *                    256 x {128, 256} on a pair of CTAs (tcgen05 cta_group::2).
  *   split_k   : number of K slices (1..64). Slices are summed in slice order,
  *               first slice first, like the reference's outer-Kc panels
  *               (sme/v3/sme-1x4-acc-kcout.cpp:464-471, 530-558).

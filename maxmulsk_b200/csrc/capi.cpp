@@ -5,7 +5,7 @@
 // maxmulsk_sgemm_v3, maxmulsk_sgemm_v4).
 #include <cstring>
 
-#include "../../include/maxmulsk.h"
+#include "maxmulsk.h"
 #include "internal.hpp"
 #include "runtime.hpp"
 #include "tuning.hpp"

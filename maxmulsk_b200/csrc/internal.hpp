@@ -5,7 +5,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "../../include/maxmulsk.h"
+#include "maxmulsk.h"
 
 namespace mmsk {
 
@@ -55,7 +55,8 @@ struct TcArgs {
     const float* A; const float* B; float* C;
     int64_t M, K, N;
     int precision;         // MAXMULSK_PREC_3XTF32 / _BF16X6 / _BF16X9
-    int tile_n;            // 64, 128 or 256 (tile_m is 128)
+    int tile_m;            // 128 (one CTA per tile) or 256 (a CTA pair per tile)
+    int tile_n;            // 64, 128 or 256
     int split_k;           // the plan's split_k
     bool reuse_planes;     // skip the split pre-pass: planes are already in place
     void* planes;          // operand planes written by the split pre-pass
@@ -63,9 +64,11 @@ struct TcArgs {
     unsigned* counters;    // per split tile and epilogue warp (zero on entry)
     int* err;              // device error word
 };
-size_t tc_workspace_bytes(int64_t M, int64_t K, int64_t N, int precision, int tile_n, int split_k);
+size_t tc_workspace_bytes(int64_t M, int64_t K, int64_t N, int precision, int tile_m, int tile_n, int split_k);
 // Bytes of the arrival counters at the start of the partial area (to zero).
-size_t tc_counter_bytes(int64_t M, int64_t K, int64_t N, int tile_n, int split_k);
+size_t tc_counter_bytes(int64_t M, int64_t K, int64_t N, int precision, int tile_m, int tile_n, int split_k);
+// Concurrently resident work slots (SMs, or CTA pairs for 256-row tiles).
+int tc_slots(int precision, int tile_m, int tile_n);
 bool tc_bind_workspace(TcArgs& a, void* ws, size_t ws_bytes);
 cudaError_t tc_launch(const TcArgs& a, cudaStream_t s);
 

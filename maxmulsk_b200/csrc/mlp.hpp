@@ -3,7 +3,7 @@
 
 #include <cstddef>
 
-#include "../../include/maxmulsk.h"
+#include "maxmulsk.h"
 
 namespace mmsk {
 

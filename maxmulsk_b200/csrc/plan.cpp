@@ -42,8 +42,10 @@ maxmulsk_status classify_plan(size_t M, size_t K, size_t N, const maxmulsk_plan*
         return MAXMULSK_OK;
     }
     if (is_tc(p.precision)) {
-        if (p.tile_m != 128 || (p.tile_n != 64 && p.tile_n != 128 && p.tile_n != 256)) {
-            set_error_message("tensor-core tiles: 128x64, 128x128 or 128x256");
+        const bool single = p.tile_m == 128 && (p.tile_n == 64 || p.tile_n == 128 || p.tile_n == 256);
+        const bool pair = p.tile_m == 256 && (p.tile_n == 128 || p.tile_n == 256);
+        if (!single && !pair) {
+            set_error_message("tensor-core tiles: 128x64, 128x128, 128x256 (one CTA), 256x128, 256x256 (CTA pair)");
             return MAXMULSK_ERR_UNSUPPORTED;
         }
         if (p.variant != MAXMULSK_TC_SPLIT_INPUTS && p.variant != MAXMULSK_TC_REUSE_PLANES) {
@@ -62,7 +64,7 @@ size_t workspace_bytes(size_t M, size_t K, size_t N, const maxmulsk_plan& p) {
     if (M == 0 || N == 0 || K == 0) return 0;
     if (p.precision == MAXMULSK_PREC_FP32)
         return simt_workspace_bytes((int64_t)M, (int64_t)K, (int64_t)N, p.tile_m, p.tile_n, p.split_k);
-    return tc_workspace_bytes((int64_t)M, (int64_t)K, (int64_t)N, p.precision, p.tile_n, p.split_k);
+    return tc_workspace_bytes((int64_t)M, (int64_t)K, (int64_t)N, p.precision, p.tile_m, p.tile_n, p.split_k);
 }
 
 // Two fixed profiles per precision, separated by shape alone, like the v4c

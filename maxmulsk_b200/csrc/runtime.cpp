@@ -145,6 +145,7 @@ maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t
     a.A = dA; a.B = dB; a.C = dC;
     a.M = (int64_t)M; a.K = (int64_t)K; a.N = (int64_t)N;
     a.precision = plan.precision;
+    a.tile_m = plan.tile_m;
     a.tile_n = plan.tile_n;
     a.reuse_planes = (plan.variant == MAXMULSK_TC_REUSE_PLANES);
     a.split_k = plan.split_k;
@@ -154,7 +155,8 @@ maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t
         return MAXMULSK_ERR_INVALID;
     }
     if (a.counters) {
-        const size_t cb = tc_counter_bytes((int64_t)M, (int64_t)K, (int64_t)N, plan.tile_n, plan.split_k);
+        const size_t cb = tc_counter_bytes((int64_t)M, (int64_t)K, (int64_t)N, plan.precision, plan.tile_m,
+                                         plan.tile_n, plan.split_k);
         st = cuda_status(cudaMemsetAsync(a.counters, 0, cb, s), "cudaMemsetAsync(counters)");
         if (st != MAXMULSK_OK) return st;
     }

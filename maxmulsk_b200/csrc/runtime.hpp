@@ -7,7 +7,7 @@
 #include <string>
 #include <cuda_runtime.h>
 
-#include "../../include/maxmulsk.h"
+#include "maxmulsk.h"
 
 namespace mmsk {
 

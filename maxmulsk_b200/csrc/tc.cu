@@ -46,12 +46,16 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <map>
 #include <mutex>
+#include <tuple>
 
 #include "internal.hpp"
 #include "sm100.cuh"
 
 namespace mmsk {
+int tc_slots(int precision, int tile_m, int tile_n);
+
 namespace {
 
 using namespace sm100;
@@ -104,6 +108,7 @@ __device__ __forceinline__ void product_planes(int mode, int q, int& pa, int& pb
 
 struct TcParams {
     int64_t M, K, N;
+    int bm;                  // rows per tile: 128, or 256 for a CTA pair
     int tiles_m, tiles_n;
     // Schedule: tiles [0, main_tiles) are cut into main_splits K slices of
     // main_kchunk; tiles [main_tiles, tiles) into tail_splits slices of
@@ -396,6 +401,285 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     }
 }
 
+// ============================================================================
+// CTA-pair variant (tcgen05 cta_group::2). Two CTAs of a cluster share one
+// 256 x BN tile: each stages its own 128 rows of A and its own BN/2 columns of
+// B, the leader CTA (rank 0) issues 256 x BN x KSTEP MMAs that read both CTAs'
+// shared memory and write each CTA's 128 rows into that CTA's TMEM. Per SM
+// this halves the B operand traffic from L2 and shared memory. The epilogue is
+// the single-CTA one, per CTA. Loads are plain (no multicast); only the MMA
+// commit arrives on both CTAs' barriers.
+// ============================================================================
+template <int MODE, int BN>
+struct CfgPair {
+    static constexpr bool TF32 = (MODE == MAXMULSK_PREC_3XTF32);
+    static constexpr int P = TF32 ? 2 : 3;
+    static constexpr int ES = TF32 ? 4 : 2;
+    static constexpr int BM = 256;                   // rows per pair tile
+    static constexpr int HM = 128;                   // rows per CTA
+    static constexpr int HN = BN / 2;                // B columns per CTA
+    static constexpr int BK = 64 / ES;
+    static constexpr int KSTEP = 32 / ES;
+    static constexpr int KSTEPS = BK / KSTEP;
+    static constexpr bool B_KMAJOR = TF32;
+    static constexpr int NBE = 128 / ES;
+    static constexpr int HNBLK = HN / NBE;           // B panels per CTA (N-major B)
+    static constexpr int A_PLANE = HM * 64;
+    static constexpr int B_PLANE = BK * HN * ES;
+    static constexpr int STAGE = P * (A_PLANE + B_PLANE);
+    static constexpr int STAGES_RAW = (220 * 1024) / STAGE;
+    static constexpr int STAGES = STAGES_RAW > 8 ? 8 : STAGES_RAW;
+    static constexpr int SMEM = STAGES * STAGE + 1024;
+    static constexpr int NPROD = TF32 ? 3 : (MODE == MAXMULSK_PREC_BF16X6 ? 6 : 9);
+    static constexpr uint32_t IDESC = make_idesc(TF32 ? 2u : 1u, 256u, (uint32_t)BN, B_KMAJOR ? 0u : 1u);
+    static constexpr uint32_t TMEM_COLS = 2 * BN;
+    static constexpr int EPI = (BN >= 256) ? 8 : 4;
+    static constexpr int COLS = BN * 4 / EPI;
+    static constexpr int THREADS = 64 + 32 * EPI;
+    static_assert(STAGES >= 2, "not enough shared memory for two stages");
+    static_assert(B_KMAJOR || HN % NBE == 0, "half tile must be whole 128-byte panels");
+    static_assert(COLS % 32 == 0, "column split must be whole");
+};
+
+template <int MODE, int BN>
+__global__ void __launch_bounds__(CfgPair<MODE, BN>::THREADS, 1)
+tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                    const TcParams p) {
+    using Cf = CfgPair<MODE, BN>;
+    constexpr int COLS = Cf::COLS;
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[Cf::STAGES];
+    __shared__ __align__(8) uint64_t empty_bar[Cf::STAGES];
+    __shared__ __align__(8) uint64_t tfull_bar[2];
+    __shared__ __align__(8) uint64_t tempty_bar[2];
+    __shared__ __align__(8) uint64_t done_bar;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank() & 1u;
+    const bool leader = (rank == 0);
+    const int64_t pair = blockIdx.x >> 1;
+    const int64_t npairs = gridDim.x >> 1;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < Cf::STAGES; s++) { mbar_init(&full_bar[s], 1); mbar_init(&empty_bar[s], 1); }
+        for (int a = 0; a < 2; a++) { mbar_init(&tfull_bar[a], 1); mbar_init(&tempty_bar[a], 2 * Cf::EPI); }
+        mbar_init(&done_bar, 1);
+        abort_s = 0;
+        fence_mbar_init();
+        fence_proxy_async();
+    }
+    if (warp == 0 && lane == 0) { prefetch_tmap(&tmA); prefetch_tmap(&tmB); }
+    if (warp == 1) { tmem_alloc_pair(&tmem_base_s, Cf::TMEM_COLS); tmem_relinquish_pair(); }
+    tc_fence_before();
+    cluster_sync();                 // barriers of both CTAs initialised before any remote use
+    tc_fence_after();
+    const uint32_t tmem_base = tmem_base_s;
+
+    auto fail = [&]() {
+        atomicOr(p.err, kErrTimeout);
+        abort_s = 1;
+    };
+    auto kblocks = [&](const Unit& w) -> int64_t { return (w.kend - w.kbeg + Cf::BK - 1) / Cf::BK; };
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer (both CTAs)
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int64_t issued = 0;
+            for (int64_t u = pair; u < p.units && !abort_s; u += npairs) {
+                const Unit w = decode_unit(p, u);
+                const int64_t nkb = kblocks(w);
+                bool ok = true;
+                for (int64_t kb = 0; kb < nkb; kb++) {
+                    if (!mbar_wait_bounded(&empty_bar[stage], phase ^ 1u, p.timeout)) { fail(); ok = false; break; }
+                    if (abort_s) { ok = false; break; }
+                    uint8_t* sa = smem + (size_t)stage * Cf::STAGE;
+                    uint8_t* sb = sa + Cf::P * Cf::A_PLANE;
+                    const uint32_t bar = mapa_shared(&full_bar[stage], 0);   // the leader's barrier
+                    if (leader) mbar_arrive_expect_tx(&full_bar[stage], (uint32_t)(2 * Cf::STAGE));
+                    const int32_t k = (int32_t)(w.kbeg + kb * Cf::BK);
+                    tma_load_3d_pair(sa, &tmA, bar, k, w.tm * Cf::BM + (int32_t)rank * Cf::HM, 0);
+                    if constexpr (Cf::B_KMAJOR)
+                        tma_load_3d_pair(sb, &tmB, bar, k, w.tn * BN + (int32_t)rank * Cf::HN, 0);
+                    else
+                        tma_load_4d_pair(sb, &tmB, bar, 0, k, w.tn * (BN / Cf::NBE) + (int32_t)rank * Cf::HNBLK, 0);
+                    issued++;
+                    if (++stage == Cf::STAGES) { stage = 0; phase ^= 1u; }
+                }
+                if (!ok) break;
+            }
+            // The leader's full barriers count both CTAs' copies: wait for ours
+            // there (leader) or for the MMAs to release our stages (follower),
+            // so no copy into this CTA's shared memory is still in flight.
+            const int64_t first = issued > Cf::STAGES ? issued - Cf::STAGES : 0;
+            for (int64_t j = first; j < issued; j++) {
+                const int st = (int)(j % Cf::STAGES);
+                const uint32_t par = (uint32_t)((j / Cf::STAGES) & 1);
+                const bool okw = leader ? mbar_wait_bounded(&full_bar[st], par, p.timeout)
+                                        : mbar_wait_bounded(&empty_bar[st], par, p.timeout);
+                if (!okw) { atomicOr(p.err, kErrTimeout); abort_s = 1; }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer (leader only)
+        if (lane == 0 && leader) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int acc = 0;
+            uint32_t acc_phase = 0;
+            bool ok = true;
+            for (int64_t u = pair; u < p.units && ok && !abort_s; u += npairs) {
+                const int64_t nkb = kblocks(decode_unit(p, u));
+                for (int64_t kb0 = 0; kb0 < nkb && ok; kb0 += p.chunk_kb) {
+                    if (!mbar_wait_bounded(&tempty_bar[acc], acc_phase ^ 1u, p.timeout)) { fail(); ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+                    const int64_t kb1 = min(nkb, kb0 + (int64_t)p.chunk_kb);
+                    for (int64_t kb = kb0; kb < kb1; kb++) {
+                        if (!mbar_wait_bounded(&full_bar[stage], phase, p.timeout)) { fail(); ok = false; break; }
+                        tc_fence_after();
+                        const uint32_t a_base = smem_u32(smem + (size_t)stage * Cf::STAGE);
+                        const uint32_t b_base = a_base + Cf::P * Cf::A_PLANE;
+#pragma unroll
+                        for (int ks = 0; ks < Cf::KSTEPS; ks++) {
+#pragma unroll
+                            for (int q = 0; q < Cf::NPROD; q++) {
+                                int pa, pb;
+                                product_planes(MODE, q, pa, pb);
+                                const uint64_t adesc = make_smem_desc(
+                                    a_base + (uint32_t)(pa * Cf::A_PLANE + ks * 32), 16u, 512u, 4u);
+                                const uint64_t bdesc = Cf::B_KMAJOR
+                                    ? make_smem_desc(b_base + (uint32_t)(pb * Cf::B_PLANE + ks * 32), 16u, 512u, 4u)
+                                    : make_smem_desc(b_base + (uint32_t)(pb * Cf::B_PLANE + ks * Cf::KSTEP * 128),
+                                                     (uint32_t)(Cf::BK * 128), 1024u, 2u);
+                                const uint32_t accum = (kb > kb0 || ks > 0 || q > 0) ? 1u : 0u;
+                                if constexpr (Cf::TF32) mma_tf32_pair(d_tmem, adesc, bdesc, Cf::IDESC, accum);
+                                else mma_bf16_pair(d_tmem, adesc, bdesc, Cf::IDESC, accum);
+                            }
+                        }
+                        tc_commit_pair_multicast(&empty_bar[stage], (uint16_t)0x3);
+                        if (++stage == Cf::STAGES) { stage = 0; phase ^= 1u; }
+                    }
+                    if (!ok) break;
+                    tc_commit_pair_multicast(&tfull_bar[acc], (uint16_t)0x3);
+                    if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+                }
+            }
+            tc_commit_pair(&done_bar);
+            if (!mbar_wait_bounded(&done_bar, 0u, p.timeout)) { atomicOr(p.err, kErrTimeout); abort_s = 1; }
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue (both CTAs)
+        const int ew = warp - 2;
+        const int quarter = warp & 3;
+        const int cgroup = ew / 4;
+        const int64_t M = p.M, N = p.N;
+        const bool vec = (N % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0);
+        const uint32_t tempty_leader0 = mapa_shared(&tempty_bar[0], 0);
+        const uint32_t tempty_leader1 = mapa_shared(&tempty_bar[1], 0);
+        int acc = 0;
+        uint32_t acc_phase = 0;
+        float sum[COLS];
+        bool stop = false;
+        for (int64_t u = pair; u < p.units && !stop; u += npairs) {
+            const Unit w = decode_unit(p, u);
+            const int64_t nkb = kblocks(w);
+            for (int64_t kb0 = 0; kb0 < nkb; kb0 += p.chunk_kb) {
+                int bad = abort_s;
+                if (!bad && lane == 0) {
+                    if (!mbar_wait_bounded(&tfull_bar[acc], acc_phase, p.timeout)) { fail(); bad = 1; }
+                }
+                bad = __shfl_sync(0xffffffffu, bad, 0);
+                if (bad) { stop = true; break; }
+                tc_fence_after();
+                const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + cgroup * COLS);
+#pragma unroll
+                for (int c = 0; c < COLS; c += 16) {
+                    uint32_t r[16];
+                    tmem_ld_32x32b_x16(taddr + (uint32_t)c, r);
+                    tmem_wait_ld();
+                    if (kb0 == 0) {
+#pragma unroll
+                        for (int j = 0; j < 16; j++) sum[c + j] = __uint_as_float(r[j]);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 16; j++) sum[c + j] = __fadd_rn(sum[c + j], __uint_as_float(r[j]));
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive_cluster(acc ? tempty_leader1 : tempty_leader0);
+                if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+            }
+            if (stop) break;
+
+            const int lrow = quarter * 32 + lane;
+            const int lcol = cgroup * COLS;
+            const int64_t row = (int64_t)w.tm * Cf::BM + (int64_t)rank * Cf::HM + lrow;
+            const int64_t col0 = (int64_t)w.tn * BN + lcol;
+            if (w.sti < 0) {
+                if (row < M) {
+                    float* dst = p.C + (size_t)row * (size_t)N + (size_t)col0;
+                    if (vec && col0 + COLS <= N) {
+#pragma unroll
+                        for (int j = 0; j < COLS; j += 4)
+                            *reinterpret_cast<float4*>(dst + j) = make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < COLS; j++)
+                            if (col0 + j < N) dst[j] = sum[j];
+                    }
+                }
+                continue;
+            }
+            // K-split tile: this CTA's 128-row half is its own partial tile.
+            constexpr size_t TILE = (size_t)Cf::HM * BN;
+            const int64_t half = w.sti * 2 + rank;
+            float* part = p.partial + ((size_t)half * p.max_splits + w.z) * TILE + (size_t)lrow * BN + lcol;
+#pragma unroll
+            for (int j = 0; j < COLS; j += 4)
+                __stcg(reinterpret_cast<float4*>(part + j), make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]));
+            __threadfence();
+            __syncwarp();
+            int last = 0;
+            unsigned* ctr = p.counters + (size_t)half * Cf::EPI + ew;
+            if (lane == 0) last = (atomicAdd(ctr, 1u) == (unsigned)(w.nsplit - 1));
+            last = __shfl_sync(0xffffffffu, last, 0);
+            if (last) {
+                __threadfence();
+                const float* base = p.partial + (size_t)half * p.max_splits * TILE;
+                for (int rr = 0; rr < 32; rr++) {
+                    const int lr = quarter * 32 + rr;
+                    const int64_t grow = (int64_t)w.tm * Cf::BM + (int64_t)rank * Cf::HM + lr;
+                    if (grow >= M) break;
+                    for (int c = lane; c < COLS; c += 32) {
+                        const int64_t gcol = col0 + c;
+                        if (gcol >= N) break;
+                        const size_t off = (size_t)lr * BN + lcol + c;
+                        float v = __ldcg(base + off);
+                        for (int q = 1; q < w.nsplit; q++) v = __fadd_rn(v, __ldcg(base + (size_t)q * TILE + off));
+                        p.C[(size_t)grow * (size_t)N + (size_t)gcol] = v;
+                    }
+                }
+                if (lane == 0) *ctr = 0u;
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();                 // no CTA leaves while its peer may still touch it
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc_pair(tmem_base, Cf::TMEM_COLS);
+    }
+}
+
 // ---------------------------------------------------------------- host side
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -418,6 +702,7 @@ inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 
 // Host-side schedule of one launch (see TcParams).
 struct Sched {
+    int bm;                          // rows per tile (128, or 256 for CTA pairs)
     int64_t tiles_m, tiles_n, tiles;
     int64_t main_tiles, main_units, units;
     int main_splits, tail_splits;
@@ -430,9 +715,11 @@ struct Sched {
 // With no K split requested and a last wave that would leave SMs idle
 // (tiles = w * SMs + r, 0 < r <= SMs / 2), the r tiles of that wave are cut
 // into floor(SMs / r) K slices so the wave is shared by all SMs.
-Sched make_sched(int64_t M, int64_t K, int64_t N, int tile_n, int split_k, int sms) {
+Sched make_sched(int64_t M, int64_t K, int64_t N, int tile_m, int tile_n, int split_k, int slots) {
+    int sms = slots;
     Sched s{};
-    s.tiles_m = (M + 127) / 128;
+    s.bm = tile_m;
+    s.tiles_m = (M + tile_m - 1) / tile_m;
     s.tiles_n = (N + tile_n - 1) / tile_n;
     s.tiles = s.tiles_m * s.tiles_n;
     s.main_splits = slice_count((size_t)K, split_k);
@@ -440,7 +727,7 @@ Sched make_sched(int64_t M, int64_t K, int64_t N, int tile_n, int split_k, int s
     s.main_tiles = s.tiles;
     s.tail_splits = 1;
     s.tail_kchunk = K;
-    if (sms <= 0) sms = 148;
+    if (sms <= 0) sms = 148;                        // work slots: SMs, or resident CTA pairs
     if (s.main_splits == 1 && s.tiles > sms) {
         const int64_t r = s.tiles % sms;
         if (r > 0 && r <= sms / 2) {
@@ -466,18 +753,28 @@ Sched make_sched(int64_t M, int64_t K, int64_t N, int tile_n, int split_k, int s
     return s;
 }
 
-// K per TMEM accumulation chunk: 32, 64 or 128 as K grows, which keeps the
-// accumulation error near a constant fraction of the FP32 SIMT kernel's.
+// K per TMEM accumulation chunk. Measured on B200 (4096^3, U[-1,1)): the
+// split product's normwise error is about 0.15 + 0.37 * chunk / sqrt(K) times
+// the FP32 SIMT kernel's (0.47x at 64, 0.84x at 128, 1.6x at 256), and wide
+// exponent ranges cost up to 1.8x more; a chunk costs a TMEM drain, about 6%
+// of throughput at 64 and nothing measurable at 128. The chunk is the largest
+// power of two <= 2 * sqrt(K), clamped to [32, 256]: error near or below the
+// SIMT kernel's for every K, with the drains no more often than needed.
 int chunk_len(int64_t K) {
-    if (K >= 16384) return 128;
-    if (K >= 4096) return 64;
-    return 32;
+    int c = 32;
+    while (c < 256 && (int64_t)(2 * c) * (2 * c) <= 4 * K) c *= 2;   // 2c <= 2*sqrt(K)
+    return c;
 }
 
+// Split tiles keep one partial per 128-row half (a CTA's rows) and slice, and
+// one arrival counter per half and epilogue warp.
+size_t counter_bytes(const Sched& s) {
+    return (size_t)s.split_tiles * (s.bm / 128) * 8 * sizeof(unsigned);
+}
 size_t partial_bytes(const Sched& s, int tile_n) {
     if (s.split_tiles == 0) return 0;
-    return align256((size_t)s.split_tiles * 8 * sizeof(unsigned)) +
-           align256((size_t)s.split_tiles * s.max_splits * 128 * (size_t)tile_n * sizeof(float));
+    return align256(counter_bytes(s)) +
+           align256((size_t)s.split_tiles * (s.bm / 128) * s.max_splits * 128 * (size_t)tile_n * sizeof(float));
 }
 
 template <int MODE, int BN>
@@ -522,9 +819,10 @@ cudaError_t launch_cfg(const TcArgs& a, cudaStream_t s) {
             return cudaErrorInvalidValue;
     }
 
-    const Sched sc = make_sched(a.M, a.K, a.N, BN, a.split_k, device_sm_count());
+    const Sched sc = make_sched(a.M, a.K, a.N, 128, BN, a.split_k, tc_slots(a.precision, 128, BN));
     TcParams prm;
     prm.M = a.M; prm.K = a.K; prm.N = a.N;
+    prm.bm = 128;
     prm.tiles_m = (int)sc.tiles_m;
     prm.tiles_n = (int)sc.tiles_n;
     prm.tiles = sc.tiles;
@@ -552,8 +850,100 @@ cudaError_t launch_cfg(const TcArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int MODE, int BN>
+cudaError_t launch_cfg_pair(const TcArgs& a, cudaStream_t s) {
+    using Cf = CfgPair<MODE, BN>;
+    EncodeTiledFn enc = get_encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    const PlaneGeom g = plane_geom(a.M, a.K, a.N, a.precision);
+    char* a_planes = static_cast<char*>(a.planes);
+    char* b_planes = a_planes + (size_t)g.P * g.a_plane_bytes;
+    const CUtensorMapDataType dt = Cf::TF32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+
+    CUtensorMap tmA, tmB;
+    {
+        const cuuint64_t dims[3] = {(cuuint64_t)g.Kp, (cuuint64_t)a.M, (cuuint64_t)g.P};
+        const cuuint64_t strides[2] = {(cuuint64_t)g.Kp * Cf::ES, (cuuint64_t)g.a_plane_bytes};
+        const cuuint32_t box[3] = {(cuuint32_t)Cf::BK, (cuuint32_t)Cf::HM, (cuuint32_t)Cf::P};
+        const cuuint32_t estr[3] = {1, 1, 1};
+        if (enc(&tmA, dt, 3, a_planes, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return cudaErrorInvalidValue;
+    }
+    if constexpr (Cf::B_KMAJOR) {
+        const cuuint64_t dims[3] = {(cuuint64_t)g.Kp, (cuuint64_t)a.N, (cuuint64_t)g.P};
+        const cuuint64_t strides[2] = {(cuuint64_t)g.Kp * Cf::ES, (cuuint64_t)g.b_plane_bytes};
+        const cuuint32_t box[3] = {(cuuint32_t)Cf::BK, (cuuint32_t)Cf::HN, (cuuint32_t)Cf::P};
+        const cuuint32_t estr[3] = {1, 1, 1};
+        if (enc(&tmB, dt, 3, b_planes, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return cudaErrorInvalidValue;
+    } else {
+        const cuuint64_t npan = (cuuint64_t)(g.Np / Cf::NBE);
+        const cuuint64_t dims[4] = {(cuuint64_t)Cf::NBE, (cuuint64_t)a.K, npan, (cuuint64_t)g.P};
+        const cuuint64_t strides[3] = {128u, (cuuint64_t)a.K * 128u, (cuuint64_t)g.b_plane_bytes};
+        const cuuint32_t box[4] = {(cuuint32_t)Cf::NBE, (cuuint32_t)Cf::BK, (cuuint32_t)Cf::HNBLK, (cuuint32_t)Cf::P};
+        const cuuint32_t estr[4] = {1, 1, 1, 1};
+        if (enc(&tmB, dt, 4, b_planes, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return cudaErrorInvalidValue;
+    }
+
+    const Sched sc = make_sched(a.M, a.K, a.N, 256, BN, a.split_k, tc_slots(a.precision, 256, BN));
+    TcParams prm;
+    prm.M = a.M; prm.K = a.K; prm.N = a.N;
+    prm.bm = 256;
+    prm.tiles_m = (int)sc.tiles_m;
+    prm.tiles_n = (int)sc.tiles_n;
+    prm.tiles = sc.tiles;
+    prm.main_tiles = sc.main_tiles;
+    prm.main_units = sc.main_units;
+    prm.units = sc.units;
+    prm.main_splits = sc.main_splits;
+    prm.tail_splits = sc.tail_splits;
+    prm.main_kchunk = sc.main_kchunk;
+    prm.tail_kchunk = sc.tail_kchunk;
+    prm.max_splits = sc.max_splits;
+    prm.chunk_kb = chunk_len(a.K) / Cf::BK;
+    prm.C = a.C;
+    prm.partial = a.partial;
+    prm.counters = a.counters;
+    prm.err = a.err;
+    prm.timeout = 2000000000LL;
+    if (sc.split_tiles > 0 && (!a.partial || !a.counters)) return cudaErrorInvalidValue;
+
+    cudaError_t e = cudaFuncSetAttribute(tc_gemm_pair_kernel<MODE, BN>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::SMEM);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(2 * sc.grid), 1, 1);
+    cfg.blockDim = dim3(Cf::THREADS, 1, 1);
+    cfg.dynamicSmemBytes = Cf::SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, tc_gemm_pair_kernel<MODE, BN>, tmA, tmB, prm);
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
 template <int MODE>
 cudaError_t launch_mode(const TcArgs& a, cudaStream_t s) {
+    if (a.tile_m == 256) {
+        switch (a.tile_n) {
+            case 128: return launch_cfg_pair<MODE, 128>(a, s);
+            case 256: return launch_cfg_pair<MODE, 256>(a, s);
+            default: return cudaErrorInvalidValue;
+        }
+    }
     switch (a.tile_n) {
         case 64: return launch_cfg<MODE, 64>(a, s);
         case 128: return launch_cfg<MODE, 128>(a, s);
@@ -562,22 +952,68 @@ cudaError_t launch_mode(const TcArgs& a, cudaStream_t s) {
     }
 }
 
+template <int MODE, int BN>
+int pair_slots_for() {
+    using Cf = CfgPair<MODE, BN>;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2, 1, 1);
+    cfg.blockDim = dim3(Cf::THREADS, 1, 1);
+    cfg.dynamicSmemBytes = Cf::SMEM;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaFuncSetAttribute(tc_gemm_pair_kernel<MODE, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             Cf::SMEM) != cudaSuccess)
+        return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, tc_gemm_pair_kernel<MODE, BN>, &cfg) != cudaSuccess) return 0;
+    return n;
+}
+
 }  // namespace
 
-size_t tc_workspace_bytes(int64_t M, int64_t K, int64_t N, int precision, int tile_n, int split_k) {
+// Concurrently resident work slots of a configuration on the current device:
+// the SM count for one-CTA tiles, the number of CTA pairs that fit at once
+// for 256-row tiles (cached per device and configuration).
+int tc_slots(int precision, int tile_m, int tile_n) {
+    if (tile_m != 256) return device_sm_count();
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_tuple(dev, precision, tile_n);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int n = 0;
+    if (precision == MAXMULSK_PREC_3XTF32) n = tile_n == 256 ? pair_slots_for<MAXMULSK_PREC_3XTF32, 256>()
+                                                            : pair_slots_for<MAXMULSK_PREC_3XTF32, 128>();
+    else if (precision == MAXMULSK_PREC_BF16X6) n = tile_n == 256 ? pair_slots_for<MAXMULSK_PREC_BF16X6, 256>()
+                                                                 : pair_slots_for<MAXMULSK_PREC_BF16X6, 128>();
+    else n = tile_n == 256 ? pair_slots_for<MAXMULSK_PREC_BF16X9, 256>() : pair_slots_for<MAXMULSK_PREC_BF16X9, 128>();
+    if (n <= 0) n = device_sm_count() / 2;
+    cache[key] = n;
+    return n;
+}
+
+size_t tc_workspace_bytes(int64_t M, int64_t K, int64_t N, int precision, int tile_m, int tile_n, int split_k) {
     const PlaneGeom g = plane_geom(M, K, N, precision);
-    const Sched sc = make_sched(M, K, N, tile_n, split_k, device_sm_count());
+    const Sched sc = make_sched(M, K, N, tile_m, tile_n, split_k, tc_slots(precision, tile_m, tile_n));
     return align256((size_t)g.P * (g.a_plane_bytes + g.b_plane_bytes)) + partial_bytes(sc, tile_n);
 }
 
-size_t tc_counter_bytes(int64_t M, int64_t K, int64_t N, int tile_n, int split_k) {
-    const Sched sc = make_sched(M, K, N, tile_n, split_k, device_sm_count());
-    return (size_t)sc.split_tiles * 8 * sizeof(unsigned);
+size_t tc_counter_bytes(int64_t M, int64_t K, int64_t N, int precision, int tile_m, int tile_n, int split_k) {
+    return counter_bytes(make_sched(M, K, N, tile_m, tile_n, split_k, tc_slots(precision, tile_m, tile_n)));
 }
 
 bool tc_bind_workspace(TcArgs& a, void* ws, size_t ws_bytes) {
     const PlaneGeom g = plane_geom(a.M, a.K, a.N, a.precision);
-    const Sched sc = make_sched(a.M, a.K, a.N, a.tile_n, a.split_k, device_sm_count());
+    const Sched sc = make_sched(a.M, a.K, a.N, a.tile_m, a.tile_n, a.split_k,
+                                tc_slots(a.precision, a.tile_m, a.tile_n));
     const size_t planes = align256((size_t)g.P * (g.a_plane_bytes + g.b_plane_bytes));
     const size_t need = planes + partial_bytes(sc, a.tile_n);
     if (!ws || ws_bytes < need || (reinterpret_cast<uintptr_t>(ws) & 255) != 0) return false;
@@ -585,7 +1021,7 @@ bool tc_bind_workspace(TcArgs& a, void* ws, size_t ws_bytes) {
     a.planes = base;
     if (sc.split_tiles > 0) {
         a.counters = reinterpret_cast<unsigned*>(base + planes);
-        a.partial = reinterpret_cast<float*>(base + planes + align256((size_t)sc.split_tiles * 8 * sizeof(unsigned)));
+        a.partial = reinterpret_cast<float*>(base + planes + align256(counter_bytes(sc)));
     } else {
         a.counters = nullptr;
         a.partial = nullptr;

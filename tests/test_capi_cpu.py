@@ -44,6 +44,7 @@ def test_status_codes_keep_reference_values(built_lib):
     ((0, 64, 128, 1, 0), False), ((0, 128, 128, 0, 0), False), ((0, 128, 128, 65, 0), False),
     ((0, 128, 128, 1, 2), False), ((1, 128, 256, 1, 0), True), ((2, 128, 64, 8, 0), True),
     ((3, 128, 128, 1, 0), True), ((1, 64, 128, 1, 0), False), ((1, 128, 96, 1, 0), False),
+    ((1, 256, 256, 1, 0), True), ((2, 256, 128, 3, 0), True), ((1, 256, 64, 1, 0), False),
     ((1, 128, 128, 1, 1), True), ((1, 128, 128, 1, 2), False), ((4, 128, 128, 1, 0), False), ((-1, 128, 128, 1, 0), False),
 ])
 def test_classify(built_lib, plan, ok):

@@ -78,14 +78,17 @@ def test_split_planes_bit_exact(cuda, oracle_mod, prec, as_b, shape):
 SHAPES = [(128, 128, 128), (67, 67, 67), (20, 35, 41), (300, 520, 200), (256, 1024, 512), (1, 64, 1), (130, 16, 300)]
 
 
+TC_TILES = [(128, 64), (128, 128), (128, 256), (256, 128), (256, 256)]
+
+
 @pytest.mark.parametrize("prec", MODES)
-@pytest.mark.parametrize("tile_n", [64, 128, 256])
+@pytest.mark.parametrize("tile", TC_TILES)
 @pytest.mark.parametrize("split_k", [1, 3])
-def test_tc_gemm_vs_exact_split_product(cuda, oracle_mod, prec, tile_n, split_k):
+def test_tc_gemm_vs_exact_split_product(cuda, oracle_mod, prec, tile, split_k):
     for i, (M, K, N) in enumerate(SHAPES):
         A = oracle_mod.fill_uniform(M * K, 30 + i)
         B = oracle_mod.fill_uniform(K * N, 60 + i)
-        plan = mm.make_plan(prec, 128, tile_n, split_k)
+        plan = mm.make_plan(prec, tile[0], tile[1], split_k)
         st, C, bands = run_plan(cuda, A, B, M, K, N, plan)
         assert st == 0, mm.last_error_message()
         assert bands, ((M, K, N), plan)
@@ -116,14 +119,30 @@ def test_split_error_within_twice_simt(cuda, oracle_mod, kind):
         assert e["normwise"] <= 2 * e_simt["normwise"] + 2.0 ** -24, (kind, int(prec), e, e_simt)
 
 
-def test_split_k_deterministic(cuda, oracle_mod):
-    M, K, N = 256, 6000, 384
+@pytest.mark.parametrize("tile", [(128, 128), (256, 256)])
+def test_split_k_deterministic(cuda, oracle_mod, tile):
+    M, K, N = 300, 6000, 384
     A = oracle_mod.fill_uniform(M * K, 81)
     B = oracle_mod.fill_uniform(K * N, 82)
-    plan = mm.make_plan(mm.Precision.TF32X3, 128, 128, 8)
+    plan = mm.make_plan(mm.Precision.TF32X3, tile[0], tile[1], 8)
     _, C1, _ = run_plan(cuda, A, B, M, K, N, plan)
     _, C2, _ = run_plan(cuda, A, B, M, K, N, plan)
     assert np.array_equal(bits(C1), bits(C2))
+
+
+@pytest.mark.parametrize("prec", MODES)
+@pytest.mark.parametrize("tile", TC_TILES)
+def test_tail_wave_split_matches_whole_tiles(cuda, oracle_mod, prec, tile):
+    # 4352 x 512 x 4352 gives tile counts that leave a partial last wave, so
+    # the schedule splits the K of the tail tiles; results must stay within
+    # the same error of the exact split product as whole tiles.
+    M, K, N = 1280 + 64, 512, 2304
+    A = oracle_mod.fill_uniform(M * K, 91)
+    B = oracle_mod.fill_uniform(K * N, 92)
+    st, C, bands = run_plan(cuda, A, B, M, K, N, mm.make_plan(prec, tile[0], tile[1], 1))
+    assert st == 0 and bands
+    ideal = oracle_mod.sgemm_split_exact(A, B, M, K, N, int(prec))
+    assert np.max(np.abs(C - ideal)) <= K * 2.0 ** -22
 
 
 def test_split_device_entry_and_picker(cuda, oracle_mod):
