@@ -167,6 +167,24 @@ size_t maxmulsk_probe_split_bytes(size_t R, size_t C, int32_t precision, int32_t
 maxmulsk_status maxmulsk_probe_split_dev(const float* dX, size_t R, size_t C, int32_t precision,
                                          int32_t as_b, void* out, void* stream);
 
+/* No counterpart in the reference (whose packing buffers are allocated inside
+ * every call). For callers that cannot allocate device memory when they call:
+ * a host application that owns the device memory budget and forbids its
+ * plug-ins to call cudaMalloc, or a latency-critical loop that cannot afford
+ * cudaMalloc/cudaFree and the synchronisation they may bring. Runs an FP32
+ * plan (the SIMT kernel, any split_k) with the split-K scratch in a static
+ * device array of MAXMULSK_STATIC_SCRATCH_BYTES that the library reserves on
+ * every GPU that loads it, held until the process exits; nothing is
+ * allocated. A plan needing more scratch returns MAXMULSK_ERR_UNSUPPORTED (C
+ * untouched). The array is shared by every call on a device and keeps the last
+ * call's contents: calls that overlap on the GPU race on it. The first call
+ * on a device resolves the array's address with that device current; make it
+ * before any stream capture. Asynchronous on `stream`. */
+#define MAXMULSK_STATIC_SCRATCH_BYTES (16u << 20)
+maxmulsk_status maxmulsk_sgemm_plan_static_dev(const float* dA, const float* dB, float* dC,
+                                               size_t M, size_t K, size_t N,
+                                               const maxmulsk_plan* plan, void* stream);
+
 /* ----------------------------------------------------------------------------
  * Status, errors, device properties.
  * ------------------------------------------------------------------------- */

@@ -63,6 +63,8 @@ _SIGNATURES: dict[str, tuple] = {
     "maxmulsk_sgemm_split": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t, c_int32]),
     "maxmulsk_sgemm_split_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t,
                                            c_int32, c_void_p]),
+    "maxmulsk_sgemm_plan_static_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t,
+                                                 POINTER(Plan), c_void_p]),
     "maxmulsk_probe_split_bytes": (c_size_t, [c_size_t, c_size_t, c_int32, c_int32]),
     "maxmulsk_probe_split_dev": (c_int32, [c_void_p, c_size_t, c_size_t, c_int32, c_int32, c_void_p, c_void_p]),
     "maxmulsk_stream_status": (c_int32, [c_void_p]),

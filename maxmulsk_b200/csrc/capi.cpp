@@ -116,6 +116,12 @@ maxmulsk_status maxmulsk_sgemm_split_dev(const float* dA, const float* dB, float
                                   static_cast<cudaStream_t>(stream));
 }
 
+maxmulsk_status maxmulsk_sgemm_plan_static_dev(const float* dA, const float* dB, float* dC, size_t M, size_t K,
+                                               size_t N, const maxmulsk_plan* plan, void* stream) {
+    if (!plan) { mmsk::set_error_message("null plan"); return MAXMULSK_ERR_INVALID; }
+    return mmsk::simt_run_static_scratch(dA, dB, dC, M, K, N, *plan, static_cast<cudaStream_t>(stream));
+}
+
 size_t maxmulsk_probe_split_bytes(size_t R, size_t C, int32_t precision, int32_t as_b) {
     if (!is_split_precision(precision)) return 0;
     return mmsk::split_one_bytes((int64_t)R, (int64_t)C, precision, as_b != 0);

@@ -47,6 +47,9 @@ size_t simt_workspace_bytes(int64_t M, int64_t K, int64_t N, int tile_m, int til
 // Lays out ws into SimtArgs fields. Returns false if ws is too small.
 bool simt_bind_workspace(SimtArgs& a, int tile_m, int tile_n, void* ws, size_t ws_bytes);
 cudaError_t simt_launch(const SimtArgs& a, int tile_m, int tile_n, int variant, cudaStream_t s);
+// The SIMT plan with its split-K scratch in a static device array (no allocation).
+maxmulsk_status simt_run_static_scratch(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
+                                        const maxmulsk_plan& plan, cudaStream_t s);
 
 // ---------------------------------------------------------------------------
 // Split-precision tensor-core path (split.cu, tc.cu)

@@ -22,8 +22,10 @@
 // matrix is never touched.
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <mutex>
 
 #include "internal.hpp"
+#include "runtime.hpp"
 
 namespace mmsk {
 namespace {
@@ -278,6 +280,93 @@ cudaError_t simt_launch(const SimtArgs& a, int tile_m, int tile_n, int variant, 
     if (tile_m == 128 && tile_n == 64) return launch_tile<128, 64>(a, variant, s);
     if (tile_m == 64 && tile_n == 64) return launch_tile<64, 64>(a, variant, s);
     return cudaErrorInvalidValue;
+}
+
+// ---------------------------------------------------------------------------
+// Static-scratch variant: the split-K SIMT path with its counters and partial
+// tiles in a fixed device array instead of caller or library allocations.
+//
+// Some callers cannot allocate device memory at the point of the call: a
+// host application that owns the whole device memory budget and forbids its
+// plug-ins to call cudaMalloc, or a latency-critical loop that cannot afford
+// cudaMalloc/cudaFree (which may synchronise the device). For them this path
+// allocates nothing: the scratch lives in the array below, which the module
+// reserves on every GPU that loads this library and keeps until the process
+// exits.
+//
+// Limits and rules:
+//   * at most MAXMULSK_STATIC_SCRATCH_BYTES (16 MiB) of scratch: a plan that
+//     needs more is rejected (MAXMULSK_ERR_UNSUPPORTED), C untouched;
+//   * one array per device, shared by every call: calls that overlap on the
+//     GPU (other streams, other host threads) race on it and must be
+//     serialised by the caller;
+//   * the first call on a device resolves the array's device address
+//     (cudaGetSymbolAddress) with that device current; make that first call
+//     before any stream capture;
+//   * the array keeps the last call's contents; the arrival counters that
+//     must start at zero are cleared on the stream before every launch.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_simt_static_scratch[MAXMULSK_STATIC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+void* g_static_addr[kMaxDevices] = {};
+
+// Device address of g_simt_static_scratch on the current device, resolved
+// once per device.
+cudaError_t static_scratch_address(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_simt_static_scratch);
+        if (e != cudaSuccess) return e;
+        g_static_addr[dev] = p;
+    }
+    *out = g_static_addr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+
+maxmulsk_status simt_run_static_scratch(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
+                                        const maxmulsk_plan& plan, cudaStream_t s) {
+    maxmulsk_status st = classify_plan(M, K, N, &plan);
+    if (st != MAXMULSK_OK) return st;
+    if (plan.precision != MAXMULSK_PREC_FP32) {
+        set_error_message("the static-scratch entry runs FP32 plans only");
+        return MAXMULSK_ERR_UNSUPPORTED;
+    }
+    if (handle_empty_dev(dC, M, K, N, s, &st)) return st;
+    if (!dA || !dB || !dC) { set_error_message("null matrix pointer"); return MAXMULSK_ERR_INVALID; }
+    const size_t need = simt_workspace_bytes((int64_t)M, (int64_t)K, (int64_t)N, plan.tile_m, plan.tile_n, plan.split_k);
+    if (need > (size_t)MAXMULSK_STATIC_SCRATCH_BYTES) {
+        set_error_message("plan needs more scratch than the static maximum of MAXMULSK_STATIC_SCRATCH_BYTES (16 MiB)");
+        return MAXMULSK_ERR_UNSUPPORTED;
+    }
+    SimtArgs a{};
+    a.A = dA; a.B = dB; a.C = dC;
+    a.M = (int64_t)M; a.K = (int64_t)K; a.N = (int64_t)N;
+    a.kchunk = (int64_t)slice_len(K, plan.split_k);
+    a.splits = slice_count(K, plan.split_k);
+    if (need > 0) {
+        void* base = nullptr;
+        st = cuda_status(static_scratch_address(&base), "cudaGetSymbolAddress(static scratch)");
+        if (st != MAXMULSK_OK) return st;
+        if (!simt_bind_workspace(a, plan.tile_m, plan.tile_n, base, need)) {
+            set_error_message("static scratch binding failed");
+            return MAXMULSK_ERR_INVALID;
+        }
+        const size_t tiles = (size_t)((M + plan.tile_m - 1) / plan.tile_m) * ((N + plan.tile_n - 1) / plan.tile_n);
+        st = cuda_status(cudaMemsetAsync(a.counters, 0, tiles * sizeof(unsigned), s), "cudaMemsetAsync(counters)");
+        if (st != MAXMULSK_OK) return st;
+    }
+    return cuda_status(simt_launch(a, plan.tile_m, plan.tile_n, plan.variant, s), "sgemm_simt launch (static scratch)");
 }
 
 }  // namespace mmsk
