@@ -167,6 +167,38 @@ size_t maxmulsk_probe_split_bytes(size_t R, size_t C, int32_t precision, int32_t
 maxmulsk_status maxmulsk_probe_split_dev(const float* dX, size_t R, size_t C, int32_t precision,
                                          int32_t as_b, void* out, void* stream);
 
+/* ----------------------------------------------------------------------------
+ * Grouped launches: many independent GEMMs in one persistent kernel, captured
+ * in a CUDA graph. The counterpart of run_batch(const Gemm*, size_t)
+ * (sme/v3/sme-1x4-acc-kcout-onestream.hpp:61-63), same fields in the same
+ * order; pointers are device pointers that must stay valid while the group
+ * exists.
+ * ------------------------------------------------------------------------- */
+typedef struct {
+    const float* A;
+    const float* B;
+    float* C;
+    size_t M, K, N;
+} maxmulsk_problem;
+
+typedef struct maxmulsk_grouped_s* maxmulsk_grouped;
+
+/* Plans the group (tile shape for the group, K split per problem; group_plan
+ * may be NULL for the picker, or an FP32 plan whose split_k is 0 = per problem
+ * or > 0 = for all), uploads its tables, allocates its scratch and captures one
+ * CUDA graph. Call with the device current. */
+maxmulsk_status maxmulsk_grouped_create(const maxmulsk_problem* problems, size_t count,
+                                        const maxmulsk_plan* group_plan, maxmulsk_grouped* out);
+/* Replays the captured graph on `stream` (asynchronous). */
+maxmulsk_status maxmulsk_grouped_launch(maxmulsk_grouped g, void* stream);
+/* The plan chosen: group tile shape, per-problem split_k (count entries, may
+ * be NULL), number of work units. */
+maxmulsk_status maxmulsk_grouped_info(maxmulsk_grouped g, maxmulsk_plan* group_plan, int32_t* split_k,
+                                      size_t* units);
+void maxmulsk_grouped_destroy(maxmulsk_grouped g);
+/* One-shot: create, launch on `stream`, wait, destroy. */
+maxmulsk_status maxmulsk_sgemm_grouped_dev(const maxmulsk_problem* problems, size_t count, void* stream);
+
 /* No counterpart in the reference (whose packing buffers are allocated inside
  * every call). For callers that cannot allocate device memory when they call:
  * a host application that owns the device memory budget and forbids its

@@ -217,6 +217,48 @@ def check(status: int, where: str = "maxmulsk") -> None:
         raise MaxMulSKError(status, where)
 
 
+class Grouped:
+    """A captured grouped launch (maxmulsk_grouped_create). `problems` is a list
+    of (dA, dB, dC, M, K, N) with torch CUDA tensors or int device pointers."""
+
+    def __init__(self, problems, plan: Plan | None = None):
+        n = len(problems)
+        arr = (Problem * max(1, n))()
+        self._keep = []
+        for i, (a, b, c, M, K, N) in enumerate(problems):
+            arr[i].A = _dev_ptr(a, M * K, "A") if M * K else 0
+            arr[i].B = _dev_ptr(b, K * N, "B") if K * N else 0
+            arr[i].C = _dev_ptr(c, M * N, "C") if M * N else 0
+            arr[i].M, arr[i].K, arr[i].N = M, K, N
+            self._keep.append((a, b, c))
+        self.count = n
+        h = ctypes.c_void_p()
+        st = lib().maxmulsk_grouped_create(arr, n, ctypes.byref(plan) if plan is not None else None, ctypes.byref(h))
+        check(st, "maxmulsk_grouped_create")
+        self.handle = h
+
+    def launch(self, stream=None) -> Status:
+        return Status(lib().maxmulsk_grouped_launch(self.handle, _stream_ptr(stream)))
+
+    def info(self):
+        p = Plan()
+        sk = (ctypes.c_int32 * max(1, self.count))()
+        units = ctypes.c_size_t()
+        check(lib().maxmulsk_grouped_info(self.handle, ctypes.byref(p), sk, ctypes.byref(units)), "grouped_info")
+        return p, list(sk)[: self.count], units.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().maxmulsk_grouped_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def matmul(a, b, precision: int = Precision.FP32, plan: Plan | None = None, stream=None):
     """torch convenience: returns a new CUDA tensor C = a @ b (float32, row-major)."""
     import torch
@@ -250,5 +292,5 @@ __all__ = [
     "sgemm_v3", "sgemm_v4", "sgemm_plan", "sgemm_split",
     "sgemm_v3_dev", "sgemm_v4_dev", "sgemm_plan_dev", "sgemm_split_dev",
     "make_plan", "classify", "choose", "choose_rule", "workspace_bytes", "slice_len",
-    "stream_status", "status_string", "last_error_message", "version", "check", "matmul", "lib",
+    "stream_status", "status_string", "last_error_message", "version", "check", "matmul", "lib", "Grouped",
 ]

@@ -65,6 +65,11 @@ _SIGNATURES: dict[str, tuple] = {
                                            c_int32, c_void_p]),
     "maxmulsk_sgemm_plan_static_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t,
                                                  POINTER(Plan), c_void_p]),
+    "maxmulsk_grouped_create": (c_int32, [POINTER(Problem), c_size_t, POINTER(Plan), POINTER(c_void_p)]),
+    "maxmulsk_grouped_launch": (c_int32, [c_void_p, c_void_p]),
+    "maxmulsk_grouped_info": (c_int32, [c_void_p, POINTER(Plan), POINTER(c_int32), POINTER(c_size_t)]),
+    "maxmulsk_grouped_destroy": (None, [c_void_p]),
+    "maxmulsk_sgemm_grouped_dev": (c_int32, [POINTER(Problem), c_size_t, c_void_p]),
     "maxmulsk_probe_split_bytes": (c_size_t, [c_size_t, c_size_t, c_int32, c_int32]),
     "maxmulsk_probe_split_dev": (c_int32, [c_void_p, c_size_t, c_size_t, c_int32, c_int32, c_void_p, c_void_p]),
     "maxmulsk_stream_status": (c_int32, [c_void_p]),

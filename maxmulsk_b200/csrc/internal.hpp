@@ -47,6 +47,17 @@ size_t simt_workspace_bytes(int64_t M, int64_t K, int64_t N, int tile_m, int til
 // Lays out ws into SimtArgs fields. Returns false if ws is too small.
 bool simt_bind_workspace(SimtArgs& a, int tile_m, int tile_n, void* ws, size_t ws_bytes);
 cudaError_t simt_launch(const SimtArgs& a, int tile_m, int tile_n, int variant, cudaStream_t s);
+// Grouped launch (one persistent kernel over many problems).
+struct GroupProblem {
+    SimtArgs a;            // one problem: pointers, sizes, its K slicing and scratch
+    int32_t tiles_n;       // tiles along N (numbers the split-K counters)
+    int32_t vec;           // 128-bit loads allowed for this problem
+};
+struct GroupUnit {
+    int32_t problem, tm, tn, z;
+};
+cudaError_t simt_grouped_launch(const GroupProblem* probs, const GroupUnit* units, int nunits, unsigned* next,
+                                int tile_m, int tile_n, int variant, int grid, cudaStream_t s);
 // The SIMT plan with its split-K scratch in a static device array (no allocation).
 maxmulsk_status simt_run_static_scratch(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
                                         const maxmulsk_plan& plan, cudaStream_t s);

@@ -39,24 +39,28 @@ __device__ __forceinline__ float mac(float a, float b, float c) {
     else return __fadd_rn(c, __fmul_rn(a, b));
 }
 
-// One CTA computes a BM x BN tile of one K slice (blockIdx.z).
+// Shared-memory stages of one CTA.
+template <int BM, int BN>
+struct SimtSmem {
+    float As[2][kBK][BM + 4];                       // k-major A, padded rows
+    float Bs[2][kBK][BN];
+    int last;
+};
+
+// One CTA computes the BM x BN tile at (m0, n0) of K slice z; `tile` numbers
+// the tile for the split-K arrival counters.
 template <int BM, int BN, bool FUSED, bool VEC>
-__global__ void __launch_bounds__(kThreads, 2)
-sgemm_simt_kernel(SimtArgs p) {
+__device__ __forceinline__ void simt_tile(const SimtArgs& p, int64_t m0, int64_t n0, int z, unsigned tile,
+                                          SimtSmem<BM, BN>& sm) {
     constexpr int TM = BM / 16, TN = BN / 16;       // per-thread outputs
     constexpr int GM = TM / 4, GN = TN / 4;         // 4-wide groups per thread
     constexpr int A_F4 = BM * kBK / 4 / kThreads;   // float4 loads per thread
     constexpr int B_F4 = BN * kBK / 4 / kThreads;
-    constexpr int AP = BM + 4;                      // padded row of the k-major A stage
-
-    __shared__ __align__(16) float As[2][kBK][AP];
-    __shared__ __align__(16) float Bs[2][kBK][BN];
+    auto& As = sm.As;
+    auto& Bs = sm.Bs;
 
     const int tid = threadIdx.x;
     const int tx = tid & 15, ty = tid >> 4;
-    const int64_t m0 = (int64_t)blockIdx.y * BM;
-    const int64_t n0 = (int64_t)blockIdx.x * BN;
-    const int z = blockIdx.z;
     const int64_t kbeg = (int64_t)z * p.kchunk;
     const int64_t kend = min(p.K, kbeg + p.kchunk);
     const int64_t M = p.M, N = p.N, K = p.K;
@@ -212,14 +216,14 @@ sgemm_simt_kernel(SimtArgs p) {
     }
     __threadfence();
     __syncthreads();
-    __shared__ int s_last;
-    const unsigned tile = blockIdx.y * gridDim.x + blockIdx.x;
     if (tid == 0) {
         unsigned prev = atomicAdd(&p.counters[tile], 1u);
-        s_last = (prev == (unsigned)(p.splits - 1));
+        sm.last = (prev == (unsigned)(p.splits - 1));
     }
     __syncthreads();
-    if (!s_last) return;
+    const int last = sm.last;
+    __syncthreads();                                 // sm.last may be rewritten by the next tile
+    if (!last) return;
     __threadfence();
 #pragma unroll
     for (int i = 0; i < TM; i++) {
@@ -239,6 +243,38 @@ sgemm_simt_kernel(SimtArgs p) {
         }
     }
     if (tid == 0) p.counters[tile] = 0u;   // leave the counter ready for the next call
+}
+
+template <int BM, int BN, bool FUSED, bool VEC>
+__global__ void __launch_bounds__(kThreads, 2)
+sgemm_simt_kernel(SimtArgs p) {
+    __shared__ __align__(16) SimtSmem<BM, BN> sm;
+    simt_tile<BM, BN, FUSED, VEC>(p, (int64_t)blockIdx.y * BM, (int64_t)blockIdx.x * BN, blockIdx.z,
+                                  blockIdx.y * gridDim.x + blockIdx.x, sm);
+}
+
+// Grouped launch: one persistent kernel over a list of (problem, tile, K
+// slice) units taken from an atomic counter, heaviest units first. Each unit
+// is exactly the tile a per-GEMM launch of that problem computes, so results
+// are identical to running the problems one by one.
+template <int BM, int BN, bool FUSED>
+__global__ void __launch_bounds__(kThreads, 2)
+sgemm_simt_grouped_kernel(const GroupProblem* __restrict__ probs, const GroupUnit* __restrict__ units, int nunits,
+                          unsigned* next) {
+    __shared__ __align__(16) SimtSmem<BM, BN> sm;
+    __shared__ int s_unit;
+    for (;;) {
+        if (threadIdx.x == 0) s_unit = (int)atomicAdd(next, 1u);
+        __syncthreads();
+        const int u = s_unit;
+        __syncthreads();
+        if (u >= nunits) break;
+        const GroupUnit w = units[u];
+        const GroupProblem& P = probs[w.problem];
+        const unsigned tile = (unsigned)w.tm * (unsigned)P.tiles_n + (unsigned)w.tn;
+        if (P.vec) simt_tile<BM, BN, FUSED, true>(P.a, (int64_t)w.tm * BM, (int64_t)w.tn * BN, w.z, tile, sm);
+        else simt_tile<BM, BN, FUSED, false>(P.a, (int64_t)w.tm * BM, (int64_t)w.tn * BN, w.z, tile, sm);
+    }
 }
 
 template <int BM, int BN>
@@ -279,6 +315,26 @@ cudaError_t simt_launch(const SimtArgs& a, int tile_m, int tile_n, int variant, 
     if (tile_m == 128 && tile_n == 128) return launch_tile<128, 128>(a, variant, s);
     if (tile_m == 128 && tile_n == 64) return launch_tile<128, 64>(a, variant, s);
     if (tile_m == 64 && tile_n == 64) return launch_tile<64, 64>(a, variant, s);
+    return cudaErrorInvalidValue;
+}
+
+namespace {
+template <int BM, int BN>
+cudaError_t launch_grouped_tile(const GroupProblem* probs, const GroupUnit* units, int nunits, unsigned* next,
+                                int grid, int variant, cudaStream_t s) {
+    if (variant == MAXMULSK_FP32_SCALAR)
+        sgemm_simt_grouped_kernel<BM, BN, false><<<grid, kThreads, 0, s>>>(probs, units, nunits, next);
+    else
+        sgemm_simt_grouped_kernel<BM, BN, true><<<grid, kThreads, 0, s>>>(probs, units, nunits, next);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t simt_grouped_launch(const GroupProblem* probs, const GroupUnit* units, int nunits, unsigned* next,
+                                int tile_m, int tile_n, int variant, int grid, cudaStream_t s) {
+    if (tile_m == 128 && tile_n == 128) return launch_grouped_tile<128, 128>(probs, units, nunits, next, grid, variant, s);
+    if (tile_m == 128 && tile_n == 64) return launch_grouped_tile<128, 64>(probs, units, nunits, next, grid, variant, s);
+    if (tile_m == 64 && tile_n == 64) return launch_grouped_tile<64, 64>(probs, units, nunits, next, grid, variant, s);
     return cudaErrorInvalidValue;
 }
 

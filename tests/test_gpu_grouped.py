@@ -1,0 +1,115 @@
+"""Grouped launch (one persistent kernel over many GEMMs, replayed from a CUDA
+graph) against the oracle: every problem bit for bit equal to the oracle's
+panel sum with that problem's K split, like a per-GEMM launch; C regions
+between problems untouched; graph replays identical. The counterpart of the
+reference's run_batch (sme/v3/sme-1x4-acc-kcout-onestream.hpp:61-63)."""
+import numpy as np
+import pytest
+
+import maxmulsk_b200 as mm
+from maxmulsk_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+SENT = 3.75
+
+
+def _group(cuda, oracle_mod, shapes, seed, plan=None):
+    torch = cuda
+    problems, host, offs = [], [], []
+    total = sum(m * n for m, k, n in shapes) + 64 * (len(shapes) + 1)
+    cbuf = torch.full((total,), SENT, device="cuda")
+    off = 64
+    for i, (M, K, N) in enumerate(shapes):
+        A = oracle_mod.fill_uniform(M * K, seed + 2 * i) if M * K else np.zeros(1, np.float32)
+        B = oracle_mod.fill_uniform(K * N, seed + 2 * i + 1) if K * N else np.zeros(1, np.float32)
+        dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+        problems.append((dA, dB, cbuf.data_ptr() + 4 * off, M, K, N))
+        host.append((A, B))
+        offs.append(off)
+        off += M * N + 64
+    g = mm.Grouped(problems, plan)
+    return g, cbuf, host, offs
+
+
+def _check(cuda, oracle_mod, g, cbuf, host, offs, shapes):
+    plan, splits, _ = g.info()
+    c = cbuf.cpu().numpy()
+    mask = np.ones(c.size, bool)
+    for (M, K, N), (A, B), off, s in zip(shapes, host, offs, splits):
+        got = c[off: off + M * N].reshape(M, N)
+        mask[off: off + M * N] = False
+        if M * N == 0:
+            continue
+        if K == 0:
+            assert np.all(got == 0)
+            continue
+        want = oracle_mod.sgemm_panels(A, B, M, K, N, kc=mm.slice_len(K, s), fma=plan.variant == 0)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), ((M, K, N), s)
+    assert np.all(c[mask] == SENT), "a grouped launch wrote outside its C matrices"
+
+
+MIXED = [(1, 700, 3), (37, 5, 129), (128, 1024, 128), (67, 67, 67), (300, 2049, 90), (1, 8192, 1024),
+         (511, 640, 512), (20, 35, 41), (0, 16, 16), (16, 0, 16), (129, 4000, 257), (3, 999, 1000)]
+
+
+@pytest.mark.parametrize("tile", [None, (128, 128), (128, 64), (64, 64)])
+def test_grouped_bit_exact_and_contained(cuda, oracle_mod, tile):
+    plan = None if tile is None else mm.make_plan(0, tile[0], tile[1], 0)
+    g, cbuf, host, offs = _group(cuda, oracle_mod, MIXED, 100, plan)
+    assert g.launch() == 0
+    assert mm.stream_status() == 0
+    _check(cuda, oracle_mod, g, cbuf, host, offs, MIXED)
+    g.close()
+
+
+def test_grouped_graph_replays_identically(cuda, oracle_mod):
+    shapes = MIXED[:8]
+    g, cbuf, host, offs = _group(cuda, oracle_mod, shapes, 300)
+    assert g.launch() == 0
+    cuda.cuda.synchronize()
+    first = cbuf.clone()
+    for off, (M, K, N) in zip(offs, shapes):
+        cbuf[off: off + M * N] = -7.0
+    for _ in range(3):
+        assert g.launch() == 0
+    cuda.cuda.synchronize()
+    assert bool(cuda.equal(first, cbuf))
+    g.close()
+
+
+def test_grouped_scalar_variant_and_fixed_split(cuda, oracle_mod):
+    plan = mm.make_plan(0, 64, 64, 3, mm.FP32_SCALAR)
+    g, cbuf, host, offs = _group(cuda, oracle_mod, MIXED, 500, plan)
+    _, splits, _ = g.info()
+    assert all(s == 3 or s == 1 for s in splits)
+    assert g.launch() == 0
+    cuda.cuda.synchronize()
+    _check(cuda, oracle_mod, g, cbuf, host, offs, MIXED)
+
+
+def test_grouped_benchmark_batch_sampled(cuda, oracle_mod):
+    # The grouped batch of the benchmark (256 GEMMs); the FP64 error of a
+    # sample of problems is FP32-class and every problem's C is written.
+    torch = cuda
+    shapes = workloads.grouped_problems()
+    probs, As, Bs, Cs = [], [], [], []
+    for i, (M, K, N) in enumerate(shapes):
+        a = torch.rand(M * K, device="cuda") * 2 - 1
+        b = torch.rand(K * N, device="cuda") * 2 - 1
+        c = torch.full((M * N,), SENT, device="cuda")
+        probs.append((a, b, c, M, K, N))
+        As.append(a); Bs.append(b); Cs.append(c)
+    g = mm.Grouped(probs)
+    assert g.launch() == 0
+    assert mm.stream_status() == 0
+    rng = np.random.default_rng(0)
+    for i in rng.choice(len(shapes), 12, replace=False):
+        M, K, N = shapes[i]
+        ref = As[i].view(M, K).double() @ Bs[i].view(K, N).double()
+        err = float(torch.linalg.norm(Cs[i].view(M, N).double() - ref) /
+                    (torch.linalg.norm(As[i].double()) * torch.linalg.norm(Bs[i].double())))
+        assert err < 4 * 2.0 ** -24 * np.sqrt(K), (shapes[i], err)
+    for c in Cs:
+        assert not bool((c == SENT).any())
+    g.close()
