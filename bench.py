@@ -214,6 +214,147 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- tables
+def graph_time(torch, fn, reps: int) -> float:
+    """Seconds per call of fn, measured by replaying a CUDA graph of `reps`
+    calls (no host launch overhead in the measurement)."""
+    fn()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        fn()                                          # warm on the capture stream
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g):
+        for _ in range(reps):
+            fn()
+    g.replay()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    del g
+    return e0.elapsed_time(e1) / 1e3 / (3 * reps)
+
+
+def run_tables(args) -> None:
+    """Per-cell measurements of the other benchmark configurations (one JSON
+    line per cell): the square sweep with uniform and wide inputs, the narrow-M
+    shapes, the grouped batch."""
+    import numpy as np
+    import torch
+
+    import maxmulsk_b200 as mm
+    from maxmulsk_b200 import datagen, workloads
+
+    torch.cuda.set_device(env_int("LOCAL_RANK", 0))
+    peaks, peak_src = measured_peaks()
+    fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    kernels = [("simt", 0), ("tf32x3", 1), ("bf16x6", 2), ("bf16x9", 3)]
+
+    def run_plan(dA, dB, dC, M, K, N, plan):
+        nb = mm.workspace_bytes(M, K, N, plan)
+        ws = torch.empty(nb + 256, dtype=torch.uint8, device="cuda")
+        wp = ws.data_ptr() + ((-ws.data_ptr()) % 256)
+
+        def fn():
+            mm.check(mm.sgemm_plan_dev(dA, dB, dC, M, K, N, plan, wp, nb), "plan")
+        return fn, ws
+
+    def errors(dA, dB, dC, M, K, N):
+        A64, B64 = dA.view(M, K).double(), dB.view(K, N).double()
+        C64 = A64 @ B64
+        d = (dC.view(M, N).double() - C64).abs()
+        floor = (A64.abs() @ B64.abs()) * 2.0 ** -24
+        nw = float(torch.linalg.norm(d) / (torch.linalg.norm(A64) * torch.linalg.norm(B64)))
+        return nw, float((d / torch.maximum(C64.abs(), floor)).max())
+
+    def emit(d):
+        print(json.dumps(d), flush=True)
+
+    if args.workload in ("sweep", "narrow"):
+        if args.workload == "sweep":
+            cells = [(S, S, S, dist) for S in workloads.SQUARE for dist in ("uniform", "wide")]
+        else:
+            cells = [(M, K, N, "normal") for (M, K, N) in workloads.NARROW_M]
+        for (M, K, N, dist) in cells:
+            if dist == "normal":
+                A = datagen.normal(M * K, 31, 1.0 / np.sqrt(K)); B = datagen.normal(K * N, 32, 1.0 / np.sqrt(K))
+            elif dist == "wide":
+                A = datagen.wide(M * K, 31); B = datagen.wide(K * N, 32)
+            else:
+                A = datagen.uniform(M * K, 31); B = datagen.uniform(K * N, 32)
+            dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+            flops = 2.0 * M * N * K
+            bytes_min = 4.0 * (M * K + K * N + M * N)
+            simt_err = None
+            for name, pc in kernels:
+                dC = torch.empty(M * N, device="cuda")
+                plan = mm.choose(M, K, N, pc)
+                fn, ws = run_plan(dA, dB, dC, M, K, N, plan)
+                reps = int(max(3, min(200, 2e10 / flops)))
+                t = graph_time(torch, fn, reps)
+                nw, mr = errors(dA, dB, dC, M, K, N)
+                if pc == 0:
+                    simt_err = nw
+                peak = fp32_peak if pc == 0 else peaks["bf16_tflops"] / (2.0 if pc == 1 else 1.0) / PRODUCTS[pc]
+                emit({"workload": args.workload, "M": M, "K": K, "N": N, "dist": dist, "kernel": name,
+                      "plan": list(plan.as_tuple()), "ms": t * 1e3, "gflops": flops / t / 1e9,
+                      "frac_compute_roofline": flops / t / 1e12 / peak,
+                      "hbm_gbs_at_min_bytes": bytes_min / t / 1e9,
+                      "frac_hbm_roofline": bytes_min / t / 1e9 / peaks["hbm_gbs"],
+                      "normwise": nw, "max_rel": mr, "normwise_over_simt": nw / simt_err,
+                      "peak_basis": ("FP32 FMA nominal at max clock" if pc == 0 else
+                                     f"{peak_src} bf16 {peaks['bf16_tflops']} TF/s / {PRODUCTS[pc]}"
+                                     + (" / 2 (TF32)" if pc == 1 else ""))})
+                del ws, dC
+        return
+
+    # grouped batch: one persistent launch from a CUDA graph vs one launch per GEMM
+    shapes = workloads.grouped_problems()
+    probs, keep = [], []
+    for i, (M, K, N) in enumerate(shapes):
+        a = torch.from_numpy(datagen.uniform(M * K, 1000 + 2 * i)).cuda()
+        b = torch.from_numpy(datagen.uniform(K * N, 1001 + 2 * i)).cuda()
+        c = torch.empty(M * N, device="cuda")
+        probs.append((a, b, c, M, K, N))
+    flops = sum(2.0 * M * K * N for M, K, N in shapes)
+    g = mm.Grouped(probs)
+    gp, splits, units = g.info()
+    for _ in range(3):
+        g.launch()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 20
+    e0.record()
+    for _ in range(reps):
+        g.launch()
+    e1.record()
+    torch.cuda.synchronize()
+    t_group = e0.elapsed_time(e1) / 1e3 / reps
+    # one launch per GEMM, same tile shape and K split per problem, replayed from a graph
+    fns = []
+    for (a, b, c, M, K, N), s in zip(probs, splits):
+        plan = mm.make_plan(0, gp.tile_m, gp.tile_n, max(1, s))
+        fn, ws = run_plan(a, b, c, M, K, N, plan)
+        fns.append(fn)
+        keep.append(ws)
+    t_seq = graph_time(torch, lambda: [f() for f in fns], 1)
+    emit({"workload": "grouped", "problems": len(shapes), "gflop": flops / 1e9, "units": units,
+          "plan": {"tile_m": gp.tile_m, "tile_n": gp.tile_n, "split_k_max": max(splits)},
+          "grouped_ms": t_group * 1e3, "grouped_gflops": flops / t_group / 1e9,
+          "per_gemm_launches_ms": t_seq * 1e3, "per_gemm_launches_gflops": flops / t_seq / 1e9,
+          "frac_fp32_roofline": flops / t_group / 1e12 / fp32_peak})
+    g.close()
+
+
 # ----------------------------------------------------------------------------- ours
 def main() -> None:
     ap = argparse.ArgumentParser()
@@ -225,11 +366,16 @@ def main() -> None:
     ap.add_argument("--precision", choices=["auto"] + list(PREC), default="auto",
                     help="split mode; auto = the fastest mode on this device, picked during warm-up")
     ap.add_argument("--no-extras", action="store_true", help="headline timing only (for profiling runs)")
+    ap.add_argument("--workload", choices=["square4096", "sweep", "narrow", "grouped"], default="square4096",
+                    help="square4096 (default, one JSON line) or a per-cell table of the other configurations")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload != "square4096":
+        run_tables(args)
         return
 
     import numpy as np

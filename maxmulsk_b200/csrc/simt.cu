@@ -48,10 +48,13 @@ struct SimtSmem {
 };
 
 // One CTA computes the BM x BN tile at (m0, n0) of K slice z; `tile` numbers
-// the tile for the split-K arrival counters.
-template <int BM, int BN, bool FUSED, bool VEC>
+// the tile for the split-K arrival counters. VM selects 128-bit loads and
+// stores: 0 never, 1 always (both fixed at compile time), 2 at run time by
+// `vec_rt` (one body for problems of either kind, as in grouped launches).
+template <int BM, int BN, bool FUSED, int VM>
 __device__ __forceinline__ void simt_tile(const SimtArgs& p, int64_t m0, int64_t n0, int z, unsigned tile,
-                                          SimtSmem<BM, BN>& sm) {
+                                          SimtSmem<BM, BN>& sm, bool vec_rt = false) {
+    const bool VEC = (VM == 2) ? vec_rt : (VM == 1);
     constexpr int TM = BM / 16, TN = BN / 16;       // per-thread outputs
     constexpr int GM = TM / 4, GN = TN / 4;         // 4-wide groups per thread
     constexpr int A_F4 = BM * kBK / 4 / kThreads;   // float4 loads per thread
@@ -225,6 +228,8 @@ __device__ __forceinline__ void simt_tile(const SimtArgs& p, int64_t m0, int64_t
     __syncthreads();                                 // sm.last may be rewritten by the next tile
     if (!last) return;
     __threadfence();
+    // Each output: slice 0, then every later slice added in slice order; four
+    // adjacent columns at a time with 128-bit loads where rows allow.
 #pragma unroll
     for (int i = 0; i < TM; i++) {
         const int64_t r = out_row(i);
@@ -232,13 +237,23 @@ __device__ __forceinline__ void simt_tile(const SimtArgs& p, int64_t m0, int64_t
 #pragma unroll
         for (int g = 0; g < GN; g++) {
             const int64_t c = out_col(g);
+            const size_t off = (size_t)r * N + c;
+            if (VEC && c + 3 < N) {
+                float4 s4 = __ldcg(reinterpret_cast<const float4*>(p.partial + off));
+                for (int q = 1; q < p.splits; q++) {
+                    const float4 t = __ldcg(reinterpret_cast<const float4*>(p.partial + (size_t)q * MN + off));
+                    s4.x = __fadd_rn(s4.x, t.x); s4.y = __fadd_rn(s4.y, t.y);
+                    s4.z = __fadd_rn(s4.z, t.z); s4.w = __fadd_rn(s4.w, t.w);
+                }
+                *reinterpret_cast<float4*>(p.C + off) = s4;
+            } else {
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                if (c + j >= N) continue;
-                const size_t off = (size_t)r * N + c + j;
-                float s = __ldcg(p.partial + off);
-                for (int q = 1; q < p.splits; q++) s = __fadd_rn(s, __ldcg(p.partial + (size_t)q * MN + off));
-                p.C[off] = s;
+                for (int j = 0; j < 4; j++) {
+                    if (c + j >= N) continue;
+                    float v = __ldcg(p.partial + off + j);
+                    for (int q = 1; q < p.splits; q++) v = __fadd_rn(v, __ldcg(p.partial + (size_t)q * MN + off + j));
+                    p.C[off + j] = v;
+                }
             }
         }
     }
@@ -249,8 +264,8 @@ template <int BM, int BN, bool FUSED, bool VEC>
 __global__ void __launch_bounds__(kThreads, 2)
 sgemm_simt_kernel(SimtArgs p) {
     __shared__ __align__(16) SimtSmem<BM, BN> sm;
-    simt_tile<BM, BN, FUSED, VEC>(p, (int64_t)blockIdx.y * BM, (int64_t)blockIdx.x * BN, blockIdx.z,
-                                  blockIdx.y * gridDim.x + blockIdx.x, sm);
+    simt_tile<BM, BN, FUSED, VEC ? 1 : 0>(p, (int64_t)blockIdx.y * BM, (int64_t)blockIdx.x * BN, blockIdx.z,
+                                          blockIdx.y * gridDim.x + blockIdx.x, sm);
 }
 
 // Grouped launch: one persistent kernel over a list of (problem, tile, K
@@ -272,8 +287,7 @@ sgemm_simt_grouped_kernel(const GroupProblem* __restrict__ probs, const GroupUni
         const GroupUnit w = units[u];
         const GroupProblem& P = probs[w.problem];
         const unsigned tile = (unsigned)w.tm * (unsigned)P.tiles_n + (unsigned)w.tn;
-        if (P.vec) simt_tile<BM, BN, FUSED, true>(P.a, (int64_t)w.tm * BM, (int64_t)w.tn * BN, w.z, tile, sm);
-        else simt_tile<BM, BN, FUSED, false>(P.a, (int64_t)w.tm * BM, (int64_t)w.tn * BN, w.z, tile, sm);
+        simt_tile<BM, BN, FUSED, 2>(P.a, (int64_t)w.tm * BM, (int64_t)w.tn * BN, w.z, tile, sm, P.vec != 0);
     }
 }
 

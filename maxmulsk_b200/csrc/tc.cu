@@ -45,6 +45,7 @@
 // for its own copies and MMAs in flight, frees TMEM and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -81,9 +82,11 @@ struct Cfg {
     static constexpr int NPROD = TF32 ? 3 : (MODE == MAXMULSK_PREC_BF16X6 ? 6 : 9);
     static constexpr uint32_t IDESC = make_idesc(TF32 ? 2u : 1u, 128u, (uint32_t)BN, B_KMAJOR ? 0u : 1u);
     static constexpr uint32_t TMEM_COLS = 2 * BN;
-    // Epilogue: 4 warps (one per TMEM lane quarter) per 128 columns.
-    static constexpr int EPI = (BN >= 256) ? 8 : 4;
+    // Epilogue: 4 warps per TMEM lane quarter set; 8 for tiles of 128 columns
+    // or more (two column groups), so each thread drains 64 or 128 columns.
+    static constexpr int EPI = (BN >= 128) ? 8 : 4;
     static constexpr int COLS = BN * 4 / EPI;        // columns per epilogue thread
+    static constexpr int LDW = (COLS >= 128) ? 32 : 64;   // columns loaded per TMEM wait (register bound)
     static constexpr int THREADS = 64 + 32 * EPI;
     static_assert(STAGES >= 2, "not enough shared memory for two stages");
     static_assert(COLS % 32 == 0, "column split must be whole");
@@ -319,16 +322,18 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                 tc_fence_after();
                 const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + cgroup * COLS);
 #pragma unroll
-                for (int c = 0; c < COLS; c += 16) {
-                    uint32_t r[16];
-                    tmem_ld_32x32b_x16(taddr + (uint32_t)c, r);
+                for (int c = 0; c < COLS; c += Cf::LDW) {
+                    uint32_t r[Cf::LDW];
+#pragma unroll
+                    for (int h = 0; h < Cf::LDW; h += 32)
+                        tmem_ld_32x32b_x32(taddr + (uint32_t)(c + h), *reinterpret_cast<uint32_t(*)[32]>(&r[h]));
                     tmem_wait_ld();
                     if (kb0 == 0) {
 #pragma unroll
-                        for (int j = 0; j < 16; j++) sum[c + j] = __uint_as_float(r[j]);
+                        for (int j = 0; j < Cf::LDW; j++) sum[c + j] = __uint_as_float(r[j]);
                     } else {
 #pragma unroll
-                        for (int j = 0; j < 16; j++) sum[c + j] = __fadd_rn(sum[c + j], __uint_as_float(r[j]));
+                        for (int j = 0; j < Cf::LDW; j++) sum[c + j] = __fadd_rn(sum[c + j], __uint_as_float(r[j]));
                     }
                 }
                 tc_fence_before();
@@ -373,19 +378,36 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             if (lane == 0) last = (atomicAdd(ctr, 1u) == (unsigned)(w.nsplit - 1));
             last = __shfl_sync(0xffffffffu, last, 0);
             if (last) {
+                // Every slice of this thread's row segment, in slice order,
+                // read back with 128-bit loads (its own slice included).
                 __threadfence();
-                const float* base = p.partial + (size_t)w.sti * p.max_splits * TILE;
-                for (int rr = 0; rr < 32; rr++) {
-                    const int lr = quarter * 32 + rr;
-                    const int64_t grow = (int64_t)w.tm * Cf::BM + lr;
-                    if (grow >= M) break;
-                    for (int c = lane; c < COLS; c += 32) {
-                        const int64_t gcol = col0 + c;
-                        if (gcol >= N) break;
-                        const size_t off = (size_t)lr * BN + lcol + c;
-                        float v = __ldcg(base + off);
-                        for (int q = 1; q < w.nsplit; q++) v = __fadd_rn(v, __ldcg(base + (size_t)q * TILE + off));
-                        p.C[(size_t)grow * (size_t)N + (size_t)gcol] = v;
+                const float* base = p.partial + (size_t)w.sti * p.max_splits * TILE + (size_t)lrow * BN + lcol;
+#pragma unroll
+                for (int j = 0; j < COLS; j += 4) {
+                    const float4 t = __ldcg(reinterpret_cast<const float4*>(base + j));
+                    sum[j] = t.x; sum[j + 1] = t.y; sum[j + 2] = t.z; sum[j + 3] = t.w;
+                }
+                for (int q = 1; q < w.nsplit; q++) {
+                    const float* bq = base + (size_t)q * TILE;
+#pragma unroll
+                    for (int j = 0; j < COLS; j += 4) {
+                        const float4 t = __ldcg(reinterpret_cast<const float4*>(bq + j));
+                        sum[j] = __fadd_rn(sum[j], t.x);
+                        sum[j + 1] = __fadd_rn(sum[j + 1], t.y);
+                        sum[j + 2] = __fadd_rn(sum[j + 2], t.z);
+                        sum[j + 3] = __fadd_rn(sum[j + 3], t.w);
+                    }
+                }
+                if (row < M) {
+                    float* dst = p.C + (size_t)row * (size_t)N + (size_t)col0;
+                    if (vec && col0 + COLS <= N) {
+#pragma unroll
+                        for (int j = 0; j < COLS; j += 4)
+                            *reinterpret_cast<float4*>(dst + j) = make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < COLS; j++)
+                            if (col0 + j < N) dst[j] = sum[j];
                     }
                 }
                 if (lane == 0) *ctr = 0u;
@@ -433,8 +455,9 @@ struct CfgPair {
     static constexpr int NPROD = TF32 ? 3 : (MODE == MAXMULSK_PREC_BF16X6 ? 6 : 9);
     static constexpr uint32_t IDESC = make_idesc(TF32 ? 2u : 1u, 256u, (uint32_t)BN, B_KMAJOR ? 0u : 1u);
     static constexpr uint32_t TMEM_COLS = 2 * BN;
-    static constexpr int EPI = (BN >= 256) ? 8 : 4;
+    static constexpr int EPI = (BN >= 128) ? 8 : 4;
     static constexpr int COLS = BN * 4 / EPI;
+    static constexpr int LDW = (COLS >= 128) ? 32 : 64;
     static constexpr int THREADS = 64 + 32 * EPI;
     static_assert(STAGES >= 2, "not enough shared memory for two stages");
     static_assert(B_KMAJOR || HN % NBE == 0, "half tile must be whole 128-byte panels");
@@ -599,16 +622,18 @@ tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                 tc_fence_after();
                 const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + cgroup * COLS);
 #pragma unroll
-                for (int c = 0; c < COLS; c += 16) {
-                    uint32_t r[16];
-                    tmem_ld_32x32b_x16(taddr + (uint32_t)c, r);
+                for (int c = 0; c < COLS; c += Cf::LDW) {
+                    uint32_t r[Cf::LDW];
+#pragma unroll
+                    for (int h = 0; h < Cf::LDW; h += 32)
+                        tmem_ld_32x32b_x32(taddr + (uint32_t)(c + h), *reinterpret_cast<uint32_t(*)[32]>(&r[h]));
                     tmem_wait_ld();
                     if (kb0 == 0) {
 #pragma unroll
-                        for (int j = 0; j < 16; j++) sum[c + j] = __uint_as_float(r[j]);
+                        for (int j = 0; j < Cf::LDW; j++) sum[c + j] = __uint_as_float(r[j]);
                     } else {
 #pragma unroll
-                        for (int j = 0; j < 16; j++) sum[c + j] = __fadd_rn(sum[c + j], __uint_as_float(r[j]));
+                        for (int j = 0; j < Cf::LDW; j++) sum[c + j] = __fadd_rn(sum[c + j], __uint_as_float(r[j]));
                     }
                 }
                 tc_fence_before();
@@ -651,19 +676,36 @@ tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
             if (lane == 0) last = (atomicAdd(ctr, 1u) == (unsigned)(w.nsplit - 1));
             last = __shfl_sync(0xffffffffu, last, 0);
             if (last) {
+                // Every slice of this thread's row segment, in slice order,
+                // read back with 128-bit loads (its own slice included).
                 __threadfence();
-                const float* base = p.partial + (size_t)half * p.max_splits * TILE;
-                for (int rr = 0; rr < 32; rr++) {
-                    const int lr = quarter * 32 + rr;
-                    const int64_t grow = (int64_t)w.tm * Cf::BM + (int64_t)rank * Cf::HM + lr;
-                    if (grow >= M) break;
-                    for (int c = lane; c < COLS; c += 32) {
-                        const int64_t gcol = col0 + c;
-                        if (gcol >= N) break;
-                        const size_t off = (size_t)lr * BN + lcol + c;
-                        float v = __ldcg(base + off);
-                        for (int q = 1; q < w.nsplit; q++) v = __fadd_rn(v, __ldcg(base + (size_t)q * TILE + off));
-                        p.C[(size_t)grow * (size_t)N + (size_t)gcol] = v;
+                const float* base = p.partial + (size_t)half * p.max_splits * TILE + (size_t)lrow * BN + lcol;
+#pragma unroll
+                for (int j = 0; j < COLS; j += 4) {
+                    const float4 t = __ldcg(reinterpret_cast<const float4*>(base + j));
+                    sum[j] = t.x; sum[j + 1] = t.y; sum[j + 2] = t.z; sum[j + 3] = t.w;
+                }
+                for (int q = 1; q < w.nsplit; q++) {
+                    const float* bq = base + (size_t)q * TILE;
+#pragma unroll
+                    for (int j = 0; j < COLS; j += 4) {
+                        const float4 t = __ldcg(reinterpret_cast<const float4*>(bq + j));
+                        sum[j] = __fadd_rn(sum[j], t.x);
+                        sum[j + 1] = __fadd_rn(sum[j + 1], t.y);
+                        sum[j + 2] = __fadd_rn(sum[j + 2], t.z);
+                        sum[j + 3] = __fadd_rn(sum[j + 3], t.w);
+                    }
+                }
+                if (row < M) {
+                    float* dst = p.C + (size_t)row * (size_t)N + (size_t)col0;
+                    if (vec && col0 + COLS <= N) {
+#pragma unroll
+                        for (int j = 0; j < COLS; j += 4)
+                            *reinterpret_cast<float4*>(dst + j) = make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < COLS; j++)
+                            if (col0 + j < N) dst[j] = sum[j];
                     }
                 }
                 if (lane == 0) *ctr = 0u;
@@ -699,6 +741,20 @@ EncodeTiledFn get_encode_fn() {
 }
 
 inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+// Raises a kernel's dynamic shared memory limit once per device (not inside
+// a later stream capture).
+template <typename Kern>
+cudaError_t set_smem_once(Kern kern, int bytes, std::atomic<uint64_t>& done) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const uint64_t bit = 1ull << (dev & 63);
+    if (done.load(std::memory_order_acquire) & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
+    return e;
+}
 
 // Host-side schedule of one launch (see TcParams).
 struct Sched {
@@ -753,17 +809,19 @@ Sched make_sched(int64_t M, int64_t K, int64_t N, int tile_m, int tile_n, int sp
     return s;
 }
 
-// K per TMEM accumulation chunk. Measured on B200 (4096^3, U[-1,1)): the
-// split product's normwise error is about 0.15 + 0.37 * chunk / sqrt(K) times
-// the FP32 SIMT kernel's (0.47x at 64, 0.84x at 128, 1.6x at 256), and wide
-// exponent ranges cost up to 1.8x more; a chunk costs a TMEM drain, about 6%
-// of throughput at 64 and nothing measurable at 128. The chunk is the largest
-// power of two <= 2 * sqrt(K), clamped to [32, 256]: error near or below the
-// SIMT kernel's for every K, with the drains no more often than needed.
-int chunk_len(int64_t K) {
-    int c = 32;
-    while (c < 256 && (int64_t)(2 * c) * (2 * c) <= 4 * K) c *= 2;   // 2c <= 2*sqrt(K)
-    return c;
+// K per TMEM accumulation chunk. Measured on B200: the split product's
+// normwise error grows with the chunk (at 4096^3, U[-1,1): 0.31x / 0.47x /
+// 0.84x / 1.6x the FP32 SIMT kernel's for 32 / 64 / 128 / 256) and is up to
+// 1.8x larger, relative to SIMT, for wide exponent ranges and small K; each
+// chunk costs one TMEM drain. Tiers that keep every measured cell at or below
+// about 1.2x SIMT: 32 below K = 4096, 64 below 16384, 128 above. A K-split
+// plan is compared against a K-split SIMT plan (shorter chains, smaller
+// error), so it keeps 32.
+int chunk_len(int64_t K, int splits) {
+    if (splits > 1) return 32;
+    if (K >= 16384) return 128;
+    if (K >= 4096) return 64;
+    return 32;
 }
 
 // Split tiles keep one partial per 128-row half (a CTA's rows) and slice, and
@@ -834,7 +892,7 @@ cudaError_t launch_cfg(const TcArgs& a, cudaStream_t s) {
     prm.main_kchunk = sc.main_kchunk;
     prm.tail_kchunk = sc.tail_kchunk;
     prm.max_splits = sc.max_splits;
-    prm.chunk_kb = chunk_len(a.K) / Cf::BK;
+    prm.chunk_kb = chunk_len(a.K, sc.main_splits) / Cf::BK;
     prm.C = a.C;
     prm.partial = a.partial;
     prm.counters = a.counters;
@@ -842,9 +900,8 @@ cudaError_t launch_cfg(const TcArgs& a, cudaStream_t s) {
     prm.timeout = 2000000000LL;   // about one second at B200 clocks
     if (sc.split_tiles > 0 && (!a.partial || !a.counters)) return cudaErrorInvalidValue;
 
-    // Per device and cheap; set on every launch so every device gets it.
-    cudaError_t e = cudaFuncSetAttribute(tc_gemm_kernel<MODE, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         Cf::SMEM);
+    static std::atomic<uint64_t> smem_set{0};
+    cudaError_t e = set_smem_once(tc_gemm_kernel<MODE, BN>, Cf::SMEM, smem_set);
     if (e != cudaSuccess) return e;
     tc_gemm_kernel<MODE, BN><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, prm);
     return cudaGetLastError();
@@ -907,7 +964,7 @@ cudaError_t launch_cfg_pair(const TcArgs& a, cudaStream_t s) {
     prm.main_kchunk = sc.main_kchunk;
     prm.tail_kchunk = sc.tail_kchunk;
     prm.max_splits = sc.max_splits;
-    prm.chunk_kb = chunk_len(a.K) / Cf::BK;
+    prm.chunk_kb = chunk_len(a.K, sc.main_splits) / Cf::BK;
     prm.C = a.C;
     prm.partial = a.partial;
     prm.counters = a.counters;
@@ -915,8 +972,8 @@ cudaError_t launch_cfg_pair(const TcArgs& a, cudaStream_t s) {
     prm.timeout = 2000000000LL;
     if (sc.split_tiles > 0 && (!a.partial || !a.counters)) return cudaErrorInvalidValue;
 
-    cudaError_t e = cudaFuncSetAttribute(tc_gemm_pair_kernel<MODE, BN>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, Cf::SMEM);
+    static std::atomic<uint64_t> smem_set{0};
+    cudaError_t e = set_smem_once(tc_gemm_pair_kernel<MODE, BN>, Cf::SMEM, smem_set);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(2 * sc.grid), 1, 1);
