@@ -74,6 +74,8 @@ typedef enum {
     MAXMULSK_PREC_3XTF32 = 1,   /* tensor cores: hi*hi + hi*lo + lo*hi, TF32      */
     MAXMULSK_PREC_BF16X6 = 2,   /* tensor cores: 3 BF16 limbs, pairs i+j <= 2     */
     MAXMULSK_PREC_BF16X9 = 3,   /* tensor cores: 3 BF16 limbs, all nine pairs     */
+    MAXMULSK_PREC_SPLIT_AUTO = 4, /* tensor cores, the picker chooses 3XTF32 or
+                                     BF16X6 (both within 2x the FP32 kernel's error) */
 } maxmulsk_precision;
 
 /* Kernel variants inside MAXMULSK_PREC_FP32. */
@@ -146,7 +148,8 @@ maxmulsk_status maxmulsk_sgemm_plan(const float* A, const float* B, float* C,
                                     const maxmulsk_plan* plan);
 
 /* Split-precision tensor-core GEMM, selected explicitly (the plain names stay
- * FP32 SIMT). precision is one of MAXMULSK_PREC_3XTF32 / _BF16X6 / _BF16X9. */
+ * FP32 SIMT). precision is one of MAXMULSK_PREC_3XTF32 / _BF16X6 / _BF16X9, or
+ * MAXMULSK_PREC_SPLIT_AUTO to let the picker choose the split count. */
 maxmulsk_status maxmulsk_sgemm_split(const float* A, const float* B, float* C,
                                      size_t M, size_t K, size_t N, int32_t precision);
 maxmulsk_status maxmulsk_sgemm_split_dev(const float* dA, const float* dB, float* dC,
@@ -198,6 +201,72 @@ maxmulsk_status maxmulsk_grouped_info(maxmulsk_grouped g, maxmulsk_plan* group_p
 void maxmulsk_grouped_destroy(maxmulsk_grouped g);
 /* One-shot: create, launch on `stream`, wait, destroy. */
 maxmulsk_status maxmulsk_sgemm_grouped_dev(const maxmulsk_problem* problems, size_t count, void* stream);
+
+/* ----------------------------------------------------------------------------
+ * Autotuner, tuning database and learned cost model.
+ * The reference's picker is a static table plus an environment override
+ * (sme/support/gemm_tuning.cpp:34-100) and a fixed rule
+ * (sme/v4/sme-1x4-v4c-dispatch.cpp:17-22). Here: an exhaustive autotuner over
+ * a fixed candidate list, a tuning database of its results, and a small MLP
+ * trained on its timings that predicts every candidate's log-time.
+ * Class 0 = FP32 candidates (24), class 1 = split-precision candidates (48).
+ * ------------------------------------------------------------------------- */
+#define MAXMULSK_MLP_FEATURES 7
+#define MAXMULSK_MLP_HIDDEN 64
+#define MAXMULSK_MLP_OUTPUTS 48
+#define MAXMULSK_MLP_PARAMS (7 * 64 + 64 + 64 * 64 + 64 + 64 * 48 + 48)
+
+/* The candidate plans of a class; returns how many were written (<= cap). */
+size_t maxmulsk_candidates(int32_t cls, maxmulsk_plan* out, size_t cap);
+
+/* Times each plan on one shape (device inputs, caller workspace): median of a
+ * CUDA-graph replay of `reps` calls (reps <= 0: chosen per plan). Writes
+ * microseconds per call to times_us; INFINITY for a plan the shape rejects or
+ * whose workspace exceeds ws_bytes. Synchronises `stream`. */
+maxmulsk_status maxmulsk_autotune_time_dev(const float* dA, const float* dB, float* dC,
+                                           size_t M, size_t K, size_t N,
+                                           const maxmulsk_plan* plans, size_t nplans,
+                                           void* ws, size_t ws_bytes, int32_t reps,
+                                           float* times_us, void* stream);
+
+/* Exhaustive search over the candidates for `precision` (FP32, SPLIT_AUTO, or
+ * one split mode); the best plan is returned and stored in the tuning
+ * database under (M, K, N, precision). */
+maxmulsk_status maxmulsk_autotune_dev(const float* dA, const float* dB, float* dC,
+                                      size_t M, size_t K, size_t N, int32_t precision,
+                                      void* ws, size_t ws_bytes, maxmulsk_plan* best,
+                                      float* best_us, void* stream);
+
+/* Tuning database (text; MAXMULSK_TUNING_DB is read on first use). */
+int32_t maxmulsk_tuning_load(const char* path);   /* entries read, or -1 */
+int32_t maxmulsk_tuning_save(const char* path);   /* entries written, or -1 */
+void maxmulsk_tuning_clear(void);
+
+/* Learned cost model: load weights (MAXMULSK_MODEL is read on first use);
+ * NULL unloads. */
+maxmulsk_status maxmulsk_model_load(const char* path);
+/* The model's features of a shape, and its predicted log-times on the host. */
+maxmulsk_status maxmulsk_mlp_features(size_t M, size_t K, size_t N, int32_t cls, float* out);
+maxmulsk_status maxmulsk_mlp_predict_host(size_t M, size_t K, size_t N, int32_t cls, float* out);
+
+/* Training and batched inference kernels (device pointers, float32, row-major).
+ * params: MAXMULSK_MLP_PARAMS floats W1[F][H] b1 W2[H][H] b2 W3[H][O] b3.
+ * forward: X[B][F] -> Z1, H1, Z2, H2 [B][H], Y[B][O] (Z1/Z2 may be NULL).
+ * backward: masked MSE over the entries with mask != 0, divided by `count`;
+ *   grads like params; work >= B * (O + 2H) floats; rowloss[B] squared errors.
+ * adam: one bias-corrected Adam step (step >= 1) on params.
+ * predict: Y[B][O]; with mask, best[B] = masked argmin (-1 if none);
+ *   work >= 2 * B * H floats. */
+maxmulsk_status maxmulsk_mlp_forward_dev(const float* params, const float* X, int32_t B, float* Z1, float* H1,
+                                         float* Z2, float* H2, float* Y, void* stream);
+maxmulsk_status maxmulsk_mlp_backward_dev(const float* params, const float* X, const float* Z1, const float* H1,
+                                          const float* Z2, const float* H2, const float* Y, const float* T,
+                                          const float* mask, int32_t B, float count, float* grads, float* work,
+                                          float* rowloss, void* stream);
+maxmulsk_status maxmulsk_mlp_adam_dev(float* params, const float* grads, float* m, float* v, float lr,
+                                      float beta1, float beta2, float eps, int32_t step, void* stream);
+maxmulsk_status maxmulsk_mlp_predict_dev(const float* params, const float* X, const float* mask, int32_t B,
+                                         float* work, float* Y, int32_t* best, void* stream);
 
 /* No counterpart in the reference (whose packing buffers are allocated inside
  * every call). For callers that cannot allocate device memory when they call:

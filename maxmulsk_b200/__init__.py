@@ -34,6 +34,7 @@ class Precision(enum.IntEnum):
     TF32X3 = 1
     BF16X6 = 2
     BF16X9 = 3
+    SPLIT_AUTO = 4
 
 
 FP32_FMA = 0

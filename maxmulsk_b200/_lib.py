@@ -70,6 +70,27 @@ _SIGNATURES: dict[str, tuple] = {
     "maxmulsk_grouped_info": (c_int32, [c_void_p, POINTER(Plan), POINTER(c_int32), POINTER(c_size_t)]),
     "maxmulsk_grouped_destroy": (None, [c_void_p]),
     "maxmulsk_sgemm_grouped_dev": (c_int32, [POINTER(Problem), c_size_t, c_void_p]),
+    "maxmulsk_candidates": (c_size_t, [c_int32, POINTER(Plan), c_size_t]),
+    "maxmulsk_autotune_time_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t,
+                                             POINTER(Plan), c_size_t, c_void_p, c_size_t, c_int32,
+                                             POINTER(c_float), c_void_p]),
+    "maxmulsk_autotune_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t, c_int32,
+                                        c_void_p, c_size_t, POINTER(Plan), POINTER(c_float), c_void_p]),
+    "maxmulsk_tuning_load": (c_int32, [c_char_p]),
+    "maxmulsk_tuning_save": (c_int32, [c_char_p]),
+    "maxmulsk_tuning_clear": (None, []),
+    "maxmulsk_model_load": (c_int32, [c_char_p]),
+    "maxmulsk_mlp_features": (c_int32, [c_size_t, c_size_t, c_size_t, c_int32, POINTER(c_float)]),
+    "maxmulsk_mlp_predict_host": (c_int32, [c_size_t, c_size_t, c_size_t, c_int32, POINTER(c_float)]),
+    "maxmulsk_mlp_forward_dev": (c_int32, [c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_void_p, c_void_p,
+                                           c_void_p, c_void_p]),
+    "maxmulsk_mlp_backward_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                            c_void_p, c_void_p, c_int32, c_float, c_void_p, c_void_p, c_void_p,
+                                            c_void_p]),
+    "maxmulsk_mlp_adam_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_float, c_float, c_float, c_float,
+                                        c_int32, c_void_p]),
+    "maxmulsk_mlp_predict_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_int32, c_void_p, c_void_p, c_void_p,
+                                           c_void_p]),
     "maxmulsk_probe_split_bytes": (c_size_t, [c_size_t, c_size_t, c_int32, c_int32]),
     "maxmulsk_probe_split_dev": (c_int32, [c_void_p, c_size_t, c_size_t, c_int32, c_int32, c_void_p, c_void_p]),
     "maxmulsk_stream_status": (c_int32, [c_void_p]),

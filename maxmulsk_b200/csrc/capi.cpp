@@ -27,7 +27,8 @@ maxmulsk_plan plan_v4(size_t M, size_t K, size_t N) {
 }
 
 bool is_split_precision(int32_t prec) {
-    return prec == MAXMULSK_PREC_3XTF32 || prec == MAXMULSK_PREC_BF16X6 || prec == MAXMULSK_PREC_BF16X9;
+    return prec == MAXMULSK_PREC_3XTF32 || prec == MAXMULSK_PREC_BF16X6 || prec == MAXMULSK_PREC_BF16X9 ||
+           prec == MAXMULSK_PREC_SPLIT_AUTO;
 }
 
 maxmulsk_plan plan_split(size_t M, size_t K, size_t N, int32_t prec) {

@@ -73,6 +73,7 @@ size_t workspace_bytes(size_t M, size_t K, size_t N, const maxmulsk_plan& p) {
 maxmulsk_plan choose_rule(size_t M, size_t K, size_t N, int precision, int sms) {
     maxmulsk_plan p;
     std::memset(&p, 0, sizeof(p));
+    if (precision == MAXMULSK_PREC_SPLIT_AUTO) precision = MAXMULSK_PREC_3XTF32;
     p.precision = precision;
     p.split_k = 1;
     if (sms <= 0) sms = 148;

@@ -16,8 +16,8 @@ bool tuning_predict(size_t M, size_t K, size_t N, int precision, maxmulsk_plan* 
 
 // Loads (replaces) the database from a text file; returns entries read or -1.
 int tuning_load_db(const char* path);
-// Adds or replaces one entry in memory.
-void tuning_put(size_t M, size_t K, size_t N, const maxmulsk_plan& p, double time_us);
+// Adds or replaces one entry in memory, under the requested precision `key`.
+void tuning_put(size_t M, size_t K, size_t N, int key, const maxmulsk_plan& p, double time_us);
 // Writes the in-memory database; returns entries written or -1.
 int tuning_save_db(const char* path);
 void tuning_clear();
