@@ -6,7 +6,7 @@ square 4096^3 FP32 GEMM of the square sweep (uniform [-1, 1) inputs, fixed
 seed), the shape the speed target is stated on.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--size S] [--precision tf32x3|bf16x6|bf16x9]
+                    [--size S] [--precision auto|fp32|tf32x3|bf16x6|bf16x9]
 
 Multi-GPU (torchrun, one rank per GPU): every rank multiplies its own M-row
 shard (a 4096 x 4096 block of A and the whole B); no collective touches the
@@ -363,8 +363,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--size", type=int, default=4096)
-    ap.add_argument("--precision", choices=["auto"] + list(PREC), default="auto",
-                    help="split mode; auto = the fastest mode on this device, picked during warm-up")
+    ap.add_argument("--precision", choices=["auto", "fp32"] + list(PREC), default="auto",
+                    help="split mode; auto = the fastest mode on this device, picked during warm-up; "
+                         "fp32 = the SIMT kernel as the timed step (profiling runs: no extras)")
     ap.add_argument("--no-extras", action="store_true", help="headline timing only (for profiling runs)")
     ap.add_argument("--workload", choices=["square4096", "sweep", "narrow", "grouped"], default="square4096",
                     help="square4096 (default, one JSON line) or a per-cell table of the other configurations")
@@ -453,7 +454,9 @@ def main() -> None:
                 best = (t, name)
             del keep
         args.precision = best[1]
-    prec = PREC[args.precision]
+    prec = 0 if args.precision == "fp32" else PREC[args.precision]
+    if prec == 0:
+        args.no_extras = True
 
     plan = mm.choose(M, K, N, prec)
     ws_bytes = mm.workspace_bytes(M, K, N, plan)
@@ -501,14 +504,16 @@ def main() -> None:
         "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform [-1, 1), SplitMix64)",
-        "config": {"workload": f"square {S}^3 FP32 GEMM, {args.precision} split tensor-core kernel "
-                               f"(split pre-pass + tcgen05 GEMM); per-rank M-row shard",
+        "config": {"workload": f"square {S}^3 FP32 GEMM, " + (
+                       "FP32 SIMT kernel" if prec == 0 else
+                       f"{args.precision} split tensor-core kernel (split pre-pass + tcgen05 GEMM)") +
+                       "; per-rank M-row shard",
                    "M": M, "K": K, "N": N, "precision": args.precision,
                    "plan": {"tile_m": plan.tile_m, "tile_n": plan.tile_n, "split_k": plan.split_k},
                    "l2": f"inputs larger than L2: A+B+C = {3 * S * S * 4 / 2**20:.0f} MiB, planes "
                          f"{ws_bytes / 2**20:.0f} MiB > 126 MB", "parallelism": f"replicas x{world} (M-row shards)"},
         "clocks": clocks,
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": (1 if prec == 0 else 3) * args.steps,
     }
 
     if not args.no_extras:

@@ -280,11 +280,20 @@ def matmul(a, b, precision: int = Precision.FP32, plan: Plan | None = None, stre
 
 
 def _plan_with_ws(a, b, c, M, K, N, plan, stream):
+    """sgemm_plan_dev with a fresh workspace on the current CUDA device."""
     import torch
     nb = workspace_bytes(M, K, N, plan)
-    ws = torch.empty(nb + 256, dtype=torch.uint8, device=a.device)
+    if nb == 0:
+        return sgemm_plan_dev(a, b, c, M, K, N, plan, None, 0, stream)
+    dev = a.device if hasattr(a, "device") else torch.device("cuda", torch.cuda.current_device())
+    ws = torch.empty(nb + 256, dtype=torch.uint8, device=dev)
     off = (-ws.data_ptr()) % 256
-    return sgemm_plan_dev(a, b, c, M, K, N, plan, ws.data_ptr() + off, nb, stream)
+    st = sgemm_plan_dev(a, b, c, M, K, N, plan, ws.data_ptr() + off, nb, stream)
+    if st == 0 and stream is not None:
+        # Once `ws` is dropped the caching allocator may hand its block to
+        # work on the current stream; order that after this call's kernels.
+        ws.record_stream(torch.cuda.ExternalStream(stream) if isinstance(stream, int) else stream)
+    return st
 
 
 __all__ = [

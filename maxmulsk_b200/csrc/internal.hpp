@@ -74,6 +74,8 @@ struct TcArgs {
     int split_k;           // the plan's split_k
     bool reuse_planes;     // skip the split pre-pass: planes are already in place
     void* planes;          // operand planes written by the split pre-pass
+    void* b_planes;        // B's planes split earlier (split_one as_b), or null:
+                           // then they follow A's planes in `planes`
     float* partial;        // compact partial tiles of the K-split tiles
     unsigned* counters;    // per split tile and epilogue warp (zero on entry)
     int* err;              // device error word

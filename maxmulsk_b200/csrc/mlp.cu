@@ -13,8 +13,11 @@
 // Features of a shape (M, K, N, class):
 //   ln(M), ln(N), ln(K) / ln(16384); (M, N, K mod 16) / 16; class (0 FP32, 1 split)
 // Every kernel is deterministic: reductions run in a fixed order, no atomics.
+#include <dlfcn.h>
+
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -155,6 +158,16 @@ void host_forward(const float* w, const float* x, float* y) {
     }
 }
 
+// <directory of this library>/../data/picker_model.bin
+std::string default_model_path() {
+    Dl_info info;
+    if (!dladdr(reinterpret_cast<void*>(&mlp_features), &info) || !info.dli_fname) return std::string();
+    std::string so(info.dli_fname);
+    const size_t slash = so.rfind('/');
+    const std::string dir = (slash == std::string::npos) ? std::string(".") : so.substr(0, slash);
+    return dir + "/../data/picker_model.bin";
+}
+
 bool load_file(const char* path, std::vector<float>& w) {
     FILE* f = std::fopen(path, "rb");
     if (!f) return false;
@@ -204,10 +217,17 @@ void mlp_unload() {
 bool mlp_predict_host(size_t M, size_t K, size_t N, int cls, float* y) {
     std::lock_guard<std::mutex> lk(g_model_mu);
     if (!g_env_tried) {
+        // MAXMULSK_MODEL names the weights; unset, the model shipped beside
+        // the library (data/picker_model.bin) is used if present; "" or
+        // "none" runs without a model (the rule picks).
         g_env_tried = true;
-        const char* path = std::getenv("MAXMULSK_MODEL");
+        const char* env = std::getenv("MAXMULSK_MODEL");
+        const std::string path = env ? std::string(env) : default_model_path();
         std::vector<float> w;
-        if (path && *path && load_file(path, w)) { g_model.w = std::move(w); g_model.loaded = true; }
+        if (!path.empty() && path != "none" && load_file(path.c_str(), w)) {
+            g_model.w = std::move(w);
+            g_model.loaded = true;
+        }
     }
     if (!g_model.loaded) return false;
     float x[F];
@@ -223,12 +243,16 @@ bool mlp_predict_plan(size_t M, size_t K, size_t N, int precision, maxmulsk_plan
     if (!mlp_predict_host(M, K, N, cls, y)) return false;
     maxmulsk_plan cands[O];
     const int n = candidate_plans(cls, cands, O);
+    const size_t max_workspace = (64u << 20) + 4 * sizeof(float) * (M * K + K * N + M * N);
     int best = -1;
     for (int i = 0; i < n; i++) {
         if (precision != MAXMULSK_PREC_FP32 && precision != MAXMULSK_PREC_SPLIT_AUTO &&
             cands[i].precision != precision)
             continue;                                              // an explicit split mode
         if (classify_plan(M, K, N, &cands[i]) != MAXMULSK_OK) continue;
+        // Plans with outsized split-K scratch were never timed (the autotuner
+        // masks them), so the model's estimate for them means nothing.
+        if (workspace_bytes(M, K, N, cands[i]) > max_workspace) continue;
         if (best < 0 || y[i] < y[best]) best = i;
     }
     if (best < 0) return false;

@@ -8,6 +8,7 @@
 // keep per-thread device copies of A, B and C.
 #include "runtime.hpp"
 
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -72,12 +73,19 @@ DeviceState* current_state() {
     return device_state(dev);
 }
 
-// Per-thread device copies for the host-pointer entry points.
+// Per-thread device copies for the host-pointer entry points, and the
+// streams and events of the row-block pipeline.
+constexpr int kPipeBlocks = 8;
 struct HostStage {
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;           // GEMM
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t b_in = nullptr;
+    cudaEvent_t a_in[kPipeBlocks] = {};
+    cudaEvent_t c_done[kPipeBlocks] = {};
     float* dA = nullptr; size_t capA = 0;
     float* dB = nullptr; size_t capB = 0;
     float* dC = nullptr; size_t capC = 0;
+    float* dBp = nullptr; size_t capBp = 0;  // B's split planes (as floats)
 };
 thread_local std::map<int, HostStage> t_stage;
 
@@ -106,7 +114,8 @@ bool handle_empty_dev(float* dC, size_t M, size_t K, size_t N, cudaStream_t s, m
 }
 
 maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
-                             const maxmulsk_plan& plan, void* ws, size_t ws_bytes, cudaStream_t s) {
+                             const maxmulsk_plan& plan, void* ws, size_t ws_bytes, cudaStream_t s,
+                             void* b_planes) {
     maxmulsk_status st = classify_plan(M, K, N, &plan);
     if (st != MAXMULSK_OK) return st;
     if (handle_empty_dev(dC, M, K, N, s, &st)) return st;
@@ -150,6 +159,7 @@ maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t
     a.reuse_planes = (plan.variant == MAXMULSK_TC_REUSE_PLANES);
     a.split_k = plan.split_k;
     a.err = ds->err_word;
+    a.b_planes = a.reuse_planes ? nullptr : b_planes;
     if (!tc_bind_workspace(a, ws, ws_bytes)) {
         set_error_message("workspace too small for the tensor-core plan");
         return MAXMULSK_ERR_INVALID;
@@ -164,7 +174,7 @@ maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t
 }
 
 maxmulsk_status run_plan_managed(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
-                                 const maxmulsk_plan& plan, cudaStream_t s) {
+                                 const maxmulsk_plan& plan, cudaStream_t s, void* b_planes) {
     maxmulsk_status st = classify_plan(M, K, N, &plan);
     if (st != MAXMULSK_OK) return st;
     if (handle_empty_dev(dC, M, K, N, s, &st)) return st;
@@ -195,7 +205,7 @@ maxmulsk_status run_plan_managed(const float* dA, const float* dB, float* dC, si
         ws = w.ptr;
         ws_bytes = w.bytes;
     }
-    return run_plan_dev(dA, dB, dC, M, K, N, plan, ws, ws_bytes, s);
+    return run_plan_dev(dA, dB, dC, M, K, N, plan, ws, ws_bytes, s, b_planes);
 }
 
 maxmulsk_status stream_status(cudaStream_t s) {
@@ -213,6 +223,101 @@ maxmulsk_status stream_status(cudaStream_t s) {
     }
     return MAXMULSK_OK;
 }
+
+namespace {
+
+bool page_locked(const void* p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+maxmulsk_status ensure_pipeline(HostStage& hs) {
+    maxmulsk_status st = MAXMULSK_OK;
+    if (!hs.h2d) st = cuda_status(cudaStreamCreateWithFlags(&hs.h2d, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (st == MAXMULSK_OK && !hs.d2h)
+        st = cuda_status(cudaStreamCreateWithFlags(&hs.d2h, cudaStreamNonBlocking), "cudaStreamCreate");
+    if (st == MAXMULSK_OK && !hs.b_in) st = cuda_status(cudaEventCreateWithFlags(&hs.b_in, cudaEventDisableTiming), "cudaEventCreate");
+    for (int i = 0; i < kPipeBlocks && st == MAXMULSK_OK; i++) {
+        if (!hs.a_in[i]) st = cuda_status(cudaEventCreateWithFlags(&hs.a_in[i], cudaEventDisableTiming), "cudaEventCreate");
+        if (st == MAXMULSK_OK && !hs.c_done[i])
+            st = cuda_status(cudaEventCreateWithFlags(&hs.c_done[i], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    return st;
+}
+
+// Row-block pipeline. B is copied first; A is copied in kPipeBlocks row
+// blocks on one copy stream, each block's GEMM starts when its rows have
+// arrived, and each block of C goes back on a second copy stream as soon as
+// it is written. The PCIe link carries A in one direction while it carries C
+// in the other, so the call costs about copy(B) + copy(A) + one block,
+// instead of copy(A, B) + GEMM + copy(C). Each row of C is the same
+// computation as in a whole-matrix launch of the same plan (the K slicing
+// does not depend on M); only the tensor-core schedule's tail-wave K split,
+// which depends on the tile count, can differ.
+maxmulsk_status host_pipelined(HostStage& hs, const float* A, const float* B, float* C, size_t M, size_t K,
+                               size_t N, const maxmulsk_plan& plan) {
+    maxmulsk_status st = ensure_pipeline(hs);
+    if (st != MAXMULSK_OK) return st;
+    size_t rows = (M + kPipeBlocks - 1) / kPipeBlocks;
+    rows = (rows + 255) / 256 * 256;
+    const int nblk = (int)((M + rows - 1) / rows);
+    cudaStream_t s = hs.stream;
+    auto fail = [&](maxmulsk_status e) {
+        cudaStreamSynchronize(hs.h2d);
+        cudaStreamSynchronize(s);
+        cudaStreamSynchronize(hs.d2h);
+        return e;
+    };
+
+    st = cuda_status(cudaMemcpyAsync(hs.dB, B, K * N * sizeof(float), cudaMemcpyHostToDevice, hs.h2d), "copy B");
+    if (st != MAXMULSK_OK) return fail(st);
+    st = cuda_status(cudaEventRecord(hs.b_in, hs.h2d), "cudaEventRecord");
+    if (st != MAXMULSK_OK) return fail(st);
+    for (int i = 0; i < nblk; i++) {
+        const size_t r0 = (size_t)i * rows, mb = std::min(rows, M - r0);
+        st = cuda_status(cudaMemcpyAsync(hs.dA + r0 * K, A + r0 * K, mb * K * sizeof(float), cudaMemcpyHostToDevice,
+                                         hs.h2d), "copy A block");
+        if (st != MAXMULSK_OK) return fail(st);
+        st = cuda_status(cudaEventRecord(hs.a_in[i], hs.h2d), "cudaEventRecord");
+        if (st != MAXMULSK_OK) return fail(st);
+    }
+
+    st = cuda_status(cudaStreamWaitEvent(s, hs.b_in, 0), "cudaStreamWaitEvent");
+    if (st != MAXMULSK_OK) return fail(st);
+    void* b_planes = nullptr;
+    if (plan.precision != MAXMULSK_PREC_FP32) {
+        // B's planes once for all blocks.
+        const size_t nb = split_one_bytes((int64_t)K, (int64_t)N, plan.precision, true);
+        st = cuda_status(grow(&hs.dBp, &hs.capBp, (nb + sizeof(float) - 1) / sizeof(float)), "cudaMalloc(B planes)");
+        if (st != MAXMULSK_OK) return fail(st);
+        st = cuda_status(split_one(hs.dB, (int64_t)K, (int64_t)N, plan.precision, true, hs.dBp, s), "split B");
+        if (st != MAXMULSK_OK) return fail(st);
+        b_planes = hs.dBp;
+    }
+    for (int i = 0; i < nblk; i++) {
+        const size_t r0 = (size_t)i * rows, mb = std::min(rows, M - r0);
+        st = cuda_status(cudaStreamWaitEvent(s, hs.a_in[i], 0), "cudaStreamWaitEvent");
+        if (st != MAXMULSK_OK) return fail(st);
+        st = run_plan_managed(hs.dA + r0 * K, hs.dB, hs.dC + r0 * N, mb, K, N, plan, s, b_planes);
+        if (st != MAXMULSK_OK) return fail(st);
+        st = cuda_status(cudaEventRecord(hs.c_done[i], s), "cudaEventRecord");
+        if (st != MAXMULSK_OK) return fail(st);
+        st = cuda_status(cudaStreamWaitEvent(hs.d2h, hs.c_done[i], 0), "cudaStreamWaitEvent");
+        if (st != MAXMULSK_OK) return fail(st);
+        st = cuda_status(cudaMemcpyAsync(C + r0 * N, hs.dC + r0 * N, mb * N * sizeof(float), cudaMemcpyDeviceToHost,
+                                         hs.d2h), "copy C block");
+        if (st != MAXMULSK_OK) return fail(st);
+    }
+    st = cuda_status(cudaStreamSynchronize(hs.d2h), "cudaStreamSynchronize");
+    if (st != MAXMULSK_OK) return fail(st);
+    return stream_status(s);
+}
+
+}  // namespace
 
 maxmulsk_status run_plan_host(const float* A, const float* B, float* C, size_t M, size_t K, size_t N,
                               const maxmulsk_plan& plan) {
@@ -234,6 +339,13 @@ maxmulsk_status run_plan_host(const float* A, const float* B, float* C, size_t M
     if ((st = cuda_status(grow(&hs.dA, &hs.capA, M * K), "cudaMalloc(A)")) != MAXMULSK_OK) return st;
     if ((st = cuda_status(grow(&hs.dB, &hs.capB, K * N), "cudaMalloc(B)")) != MAXMULSK_OK) return st;
     if ((st = cuda_status(grow(&hs.dC, &hs.capC, M * N), "cudaMalloc(C)")) != MAXMULSK_OK) return st;
+
+    // The pipeline pays off once the copies dominate; it needs page-locked A
+    // and C, since copies from pageable memory do not overlap with anything.
+    const size_t streamed = (M * K + M * N) * sizeof(float);
+    const bool planes_given = plan.precision != MAXMULSK_PREC_FP32 && plan.variant == MAXMULSK_TC_REUSE_PLANES;
+    if (M >= 1024 && streamed >= (32u << 20) && !planes_given && page_locked(A) && page_locked(C))
+        return host_pipelined(hs, A, B, C, M, K, N, plan);
 
     cudaStream_t s = hs.stream;
     st = cuda_status(cudaMemcpyAsync(hs.dA, A, M * K * sizeof(float), cudaMemcpyHostToDevice, s), "copy A");

@@ -25,14 +25,19 @@ maxmulsk_plan choose_tuned(size_t M, size_t K, size_t N, int precision, int sms)
 bool parse_config_env(maxmulsk_plan& out);
 
 // Runs a validated plan on device pointers with a caller-provided workspace.
+// b_planes (split-precision plans only): B's operand planes, already written
+// by split_one(as_b); only A is split then.
 maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
-                             const maxmulsk_plan& plan, void* ws, size_t ws_bytes, cudaStream_t s);
+                             const maxmulsk_plan& plan, void* ws, size_t ws_bytes, cudaStream_t s,
+                             void* b_planes = nullptr);
 
 // Runs a plan with the library-managed workspace of (current device, stream).
 maxmulsk_status run_plan_managed(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
-                                 const maxmulsk_plan& plan, cudaStream_t s);
+                                 const maxmulsk_plan& plan, cudaStream_t s, void* b_planes = nullptr);
 
 // Host-pointer form: copy in, run, copy out, wait, check the error word.
+// Large products with page-locked A and C run as a pipeline of row blocks, so
+// that copies in, the GEMM and copies out overlap.
 maxmulsk_status run_plan_host(const float* A, const float* B, float* C, size_t M, size_t K, size_t N,
                               const maxmulsk_plan& plan);
 

@@ -842,7 +842,7 @@ cudaError_t launch_cfg(const TcArgs& a, cudaStream_t s) {
     if (!enc) return cudaErrorNotSupported;
     const PlaneGeom g = plane_geom(a.M, a.K, a.N, a.precision);
     char* a_planes = static_cast<char*>(a.planes);
-    char* b_planes = a_planes + (size_t)g.P * g.a_plane_bytes;
+    char* b_planes = a.b_planes ? static_cast<char*>(a.b_planes) : a_planes + (size_t)g.P * g.a_plane_bytes;
     const CUtensorMapDataType dt = Cf::TF32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
 
     CUtensorMap tmA, tmB;
@@ -914,7 +914,7 @@ cudaError_t launch_cfg_pair(const TcArgs& a, cudaStream_t s) {
     if (!enc) return cudaErrorNotSupported;
     const PlaneGeom g = plane_geom(a.M, a.K, a.N, a.precision);
     char* a_planes = static_cast<char*>(a.planes);
-    char* b_planes = a_planes + (size_t)g.P * g.a_plane_bytes;
+    char* b_planes = a.b_planes ? static_cast<char*>(a.b_planes) : a_planes + (size_t)g.P * g.a_plane_bytes;
     const CUtensorMapDataType dt = Cf::TF32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
 
     CUtensorMap tmA, tmB;
@@ -1088,7 +1088,9 @@ bool tc_bind_workspace(TcArgs& a, void* ws, size_t ws_bytes) {
 
 cudaError_t tc_launch(const TcArgs& a, cudaStream_t s) {
     if (!a.reuse_planes) {
-        cudaError_t e = split_launch(a.A, a.B, a.M, a.K, a.N, a.precision, a.planes, s);
+        // With B's planes supplied from outside only A is split here.
+        cudaError_t e = a.b_planes ? split_one(a.A, a.M, a.K, a.precision, false, a.planes, s)
+                                   : split_launch(a.A, a.B, a.M, a.K, a.N, a.precision, a.planes, s);
         if (e != cudaSuccess) return e;
     }
     switch (a.precision) {

@@ -38,9 +38,7 @@ def dataset(d: dict, rows) -> tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarr
     shapes = d["shapes"][rows]
     Xs, Ts, Ms, Ts_us = [], [], [], []
     for cls, key in ((0, "t_fp32"), (1, "t_split")):
-        t = d[key][rows]
-        full = np.full((len(rows), O), np.inf, np.float32)
-        full[:, : t.shape[1]] = t
+        full = _padded(d[key][rows])
         mask = np.isfinite(full).astype(np.float32)
         T = np.where(mask > 0, np.log(np.maximum(full, 1e-3)), 0.0).astype(np.float32)
         Xs.append(features(shapes, cls)); Ts.append(T); Ms.append(mask); Ts_us.append(full)
@@ -134,8 +132,14 @@ def regret(times_us: np.ndarray, picks: np.ndarray) -> dict:
             "total_time": float(t[ok].sum() / best[ok].sum() - 1.0)}
 
 
+def _padded(t: np.ndarray) -> np.ndarray:
+    full = np.full((t.shape[0], O), np.inf, np.float32)
+    full[:, : t.shape[1]] = t
+    return full
+
+
 def rule_regret(d: dict, rows) -> dict:
-    times = np.concatenate([d["t_fp32"][rows], d["t_split"][rows]], axis=0)
+    times = np.concatenate([_padded(d["t_fp32"][rows]), _padded(d["t_split"][rows])], axis=0)
     rule = np.concatenate([d["t_rule_fp32"][rows], d["t_rule_split"][rows]])
     best = np.min(times, axis=1)
     ok = np.isfinite(best) & np.isfinite(rule)
@@ -145,7 +149,7 @@ def rule_regret(d: dict, rows) -> dict:
             "within_5pct": float((r <= 0.05).mean()), "total_time": float(rule[ok].sum() / best[ok].sum() - 1.0)}
 
 
-def train_and_evaluate(d: dict, steps: int = 3000, seed: int = 0, lr: float = 3e-3):
+def train_and_evaluate(d: dict, steps: int = 5000, seed: int = 0, lr: float = 1e-2):
     n_train = int(d["n_train"])
     tr = np.arange(n_train)
     te = np.arange(n_train, len(d["shapes"]))
@@ -162,10 +166,11 @@ def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--data", required=True)
     ap.add_argument("--out", required=True)
-    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--steps", type=int, default=5000)
+    ap.add_argument("--lr", type=float, default=1e-2)
     a = ap.parse_args()
     d = dict(np.load(a.data))
-    trainer, losses, r_mlp, r_rule = train_and_evaluate(d, steps=a.steps)
+    trainer, losses, r_mlp, r_rule = train_and_evaluate(d, steps=a.steps, lr=a.lr)
     trainer.save(a.out)
     print("loss", [round(x, 4) for x in losses])
     print("held-out regret, MLP :", r_mlp)

@@ -189,3 +189,54 @@ def test_deterministic_repeat(cuda, oracle_mod):
     _, C1, _ = run_plan(cuda, A, B, M, K, N, plan)
     _, C2, _ = run_plan(cuda, A, B, M, K, N, plan)
     assert np.array_equal(bits(C1), bits(C2))
+
+
+@pytest.mark.parametrize("prec", [mm.Precision.FP32, mm.Precision.TF32X3, mm.Precision.BF16X6])
+def test_host_entry_pipelined_path_matches_device_path(cuda, oracle_mod, prec):
+    # Page-locked A and C of >= 32 MiB with M >= 1024 take the row-block
+    # pipeline of the host entry points (B split once, A and C in blocks, a
+    # ragged last block). FP32: bit for bit the device entry's result.
+    # Split modes: the same plan on row blocks; only the tail-wave K split of
+    # the schedule may differ, so the results agree to the accumulation bound.
+    torch = cuda
+    M, K, N = 2048 + 77, 2048, 2048
+    A = oracle_mod.fill_uniform(M * K, 201)
+    B = oracle_mod.fill_uniform(K * N, 202)
+    pA = torch.from_numpy(A).pin_memory()
+    pB = torch.from_numpy(B).pin_memory()
+    pC = torch.full((M * N,), SENTINEL).pin_memory()
+    dA, dB = pA.cuda(), pB.cuda()
+    dC = torch.empty(M * N, device="cuda")
+    if prec == mm.Precision.FP32:
+        assert mm.sgemm_v3(pA.data_ptr(), pB.data_ptr(), pC.data_ptr(), M, K, N) == 0, mm.last_error_message()
+        assert mm.sgemm_v3_dev(dA, dB, dC, M, K, N) == 0
+    else:
+        assert mm.sgemm_split(pA.data_ptr(), pB.data_ptr(), pC.data_ptr(), M, K, N, prec) == 0, \
+            mm.last_error_message()
+        assert mm.sgemm_split_dev(dA, dB, dC, M, K, N, prec) == 0
+    assert mm.stream_status() == 0
+    got, want = pC.numpy(), dC.cpu().numpy()
+    if prec == mm.Precision.FP32:
+        assert np.array_equal(bits(got), bits(want))
+    else:
+        assert np.max(np.abs(got - want)) <= K * 2.0 ** -22
+        assert not np.any(got == SENTINEL)
+
+
+@pytest.mark.parametrize("world", [2, 3, 8])
+def test_row_shards_reassemble_the_product(cuda, oracle_mod, world):
+    # Each rank's M-row shard (shard.sgemm_rows_dev), run here one after the
+    # other on one device, writes exactly its rows; together they equal the
+    # whole-matrix launch bit for bit (FP32: the same chain per output).
+    from maxmulsk_b200 import shard
+    torch = cuda
+    M, K, N = 1000, 384, 200
+    A, B = _inputs(oracle_mod, M, K, N, seed=31)
+    dA, dB = to_dev(torch, A), to_dev(torch, B)
+    dC = torch.full((M * N,), SENTINEL, device="cuda")
+    whole = torch.empty(M * N, device="cuda")
+    for r in range(world):
+        assert shard.sgemm_rows_dev(dA, dB, dC, M, K, N, r, world) == 0
+    assert mm.sgemm_v3_dev(dA, dB, whole, M, K, N) == 0
+    assert mm.stream_status() == 0
+    assert bool(torch.equal(dC, whole))

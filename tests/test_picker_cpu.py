@@ -70,3 +70,33 @@ def test_candidate_lists(built_lib):
     assert {p.precision for p in c0} == {0} and {p.precision for p in c1} == {1, 2}
     for p in c0 + c1:
         assert mm.classify(512, 512, 512, p) == mm.Status.OK
+
+
+def _predict_in_fresh_process(env_value):
+    import os
+    import subprocess
+    import sys
+    env = dict(os.environ)
+    env.pop("MAXMULSK_MODEL", None)
+    if env_value is not None:
+        env["MAXMULSK_MODEL"] = env_value
+    code = ("import ctypes, maxmulsk_b200 as mm; out = (ctypes.c_float * 48)(); "
+            "print(mm.lib().maxmulsk_mlp_predict_host(4096, 4096, 4096, 1, out))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", code], env=env, cwd=root, capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    return int(r.stdout.strip())
+
+
+def test_default_model_beside_the_library(built_lib, tmp_path):
+    # Unset MAXMULSK_MODEL: the weights shipped in maxmulsk_b200/data are
+    # used; "none" turns the model off; a path names other weights.
+    import os
+    shipped = os.path.join(os.path.dirname(picker.__file__), "data", "picker_model.bin")
+    if os.path.exists(shipped):
+        assert _predict_in_fresh_process(None) == 0
+    assert _predict_in_fresh_process("none") == mm.Status.ERR_UNSUPPORTED
+    p = np.zeros(picker.NPARAM, np.float32)
+    path = str(tmp_path / "zero.bin")
+    picker.save_params(path, p)
+    assert _predict_in_fresh_process(path) == 0
