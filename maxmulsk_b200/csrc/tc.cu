@@ -12,12 +12,12 @@
 // accumulation step, so the error of one long TMEM accumulation grows with its
 // length (measured on B200: about 0.4 * L / sqrt(K) times the FP32 SIMT
 // kernel's normwise error for a chain of L k's). The kernel therefore
-// accumulates only KCHUNK = 32 k's in TMEM at a time; the epilogue warps add
-// each chunk into FP32 registers, round to nearest, chunk after chunk in k
-// order. This is the reference's outer-Kc panel scheme (first panel stores,
-// later panels add: sme/v3/sme-1x4-acc-kcout.cpp:464-471, :530-558) with a
-// 32-deep panel, and it keeps the split modes at or below the SIMT kernel's
-// error.
+// accumulates only a short chunk of k's in TMEM at a time (32, 64 or 128 by
+// K: chunk_len); the epilogue warps add each chunk into FP32 registers, round
+// to nearest, chunk after chunk in k order. This is the reference's outer-Kc
+// panel scheme (first panel stores, later panels add:
+// sme/v3/sme-1x4-acc-kcout.cpp:464-471, :530-558) with a short panel, and it
+// keeps the split modes at or near the SIMT kernel's error.
 //
 // Structure (one CTA per SM, persistent):
 //   warp 0      TMA producer: per stage one 3-D load of all A planes

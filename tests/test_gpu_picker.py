@@ -96,9 +96,11 @@ def test_trained_picker_regret_on_held_out_shapes(cuda):
     # The learned picker end to end: the MLP trained by the library's CUDA
     # forward/backward/Adam kernels on the autotuner's measured timings of
     # 2000 random shapes (M, N, K log-uniform in [1, 16384]; both classes),
-    # then judged on the 500 held-out shapes against exhaustive search. Bar:
-    # within 5% of exhaustive time (total and geometric mean), and better
-    # than the hand-written rule it replaces, timed in the same run.
+    # then judged on the 500 held-out shapes against exhaustive search (the
+    # seed is chosen on a validation part of the training shapes). Bar:
+    # within 5% of exhaustive time per shape (mean, geometric mean) and in
+    # total, and better than the hand-written rule it replaces, timed in the
+    # same run.
     import os
     d = dict(np.load(os.path.join(os.path.dirname(picker.__file__), "data", "picker_timings.npz")))
     assert int(d["n_train"]) == 2000 and len(d["shapes"]) == 2500
@@ -106,5 +108,5 @@ def test_trained_picker_regret_on_held_out_shapes(cuda):
     print("MLP", r_mlp, "rule", r_rule)
     assert losses[-1] < 0.2 * losses[0]
     assert r_mlp["rows"] == r_rule["rows"] == 1000
-    assert r_mlp["total_time"] <= 0.05 and r_mlp["geomean"] <= 0.05, r_mlp
+    assert r_mlp["mean"] <= 0.05 and r_mlp["geomean"] <= 0.05 and r_mlp["total_time"] <= 0.05, r_mlp
     assert r_mlp["total_time"] < r_rule["total_time"] and r_mlp["geomean"] < r_rule["geomean"], (r_mlp, r_rule)
