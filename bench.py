@@ -68,6 +68,17 @@ def traffic_from_profiles(name: str) -> float | None:
     return None
 
 
+def launches_per_step(plan, K: int) -> int:
+    """Kernels of this library one call of `plan` launches: the split pre-pass
+    (one per operand) and the tensor-core GEMM, or the SIMT GEMM; plus the
+    split-K reduction when every tile is cut into 3 or more K slices."""
+    import maxmulsk_b200 as mm
+    n = 1 if plan.precision == 0 else 3
+    if mm.slice_count(K, plan.split_k) >= 3:
+        n += 1
+    return n
+
+
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi clock/throttle samples while the timed region runs."""
@@ -367,6 +378,10 @@ def main() -> None:
                     help="split mode; auto = the fastest mode on this device, picked during warm-up; "
                          "fp32 = the SIMT kernel as the timed step (profiling runs: no extras)")
     ap.add_argument("--no-extras", action="store_true", help="headline timing only (for profiling runs)")
+    ap.add_argument("--shape", default=None, help="M,K,N instead of the square workload (profiling runs; "
+                                                   "implies --no-extras)")
+    ap.add_argument("--plan", default=None, help="precision,tile_m,tile_n,split_k instead of the picker's plan "
+                                                  "(profiling runs)")
     ap.add_argument("--workload", choices=["square4096", "sweep", "narrow", "grouped"], default="square4096",
                     help="square4096 (default, one JSON line) or a per-cell table of the other configurations")
     args = ap.parse_args()
@@ -397,6 +412,13 @@ def main() -> None:
 
     S = args.size
     M = K = N = S
+    if args.shape:
+        M, K, N = (int(x) for x in args.shape.split(","))
+        args.no_extras = True
+    fixed_plan = None
+    if args.plan:
+        fixed_plan = mm.make_plan(*(int(x) for x in args.plan.split(",")))
+        args.precision = {0: "fp32", 1: "tf32x3", 2: "bf16x6", 3: "bf16x9"}[fixed_plan.precision]
     # This rank's M-row shard of an (world*S) x S x S product: its own rows of A.
     A = datagen.uniform(M * K, 11 + 1000 * rank).reshape(M, K)
     B = datagen.uniform(K * N, 12).reshape(K, N)
@@ -458,7 +480,7 @@ def main() -> None:
     if prec == 0:
         args.no_extras = True
 
-    plan = mm.choose(M, K, N, prec)
+    plan = fixed_plan if fixed_plan is not None else mm.choose(M, K, N, prec)
     ws_bytes = mm.workspace_bytes(M, K, N, plan)
     ws = torch.empty(ws_bytes + 256, dtype=torch.uint8, device=dev)
     wsp = ws.data_ptr() + ((-ws.data_ptr()) % 256)
@@ -504,16 +526,16 @@ def main() -> None:
         "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded uniform [-1, 1), SplitMix64)",
-        "config": {"workload": f"square {S}^3 FP32 GEMM, " + (
+        "config": {"workload": (f"{M}x{K}x{N}" if args.shape else f"square {S}^3") + " FP32 GEMM, " + (
                        "FP32 SIMT kernel" if prec == 0 else
                        f"{args.precision} split tensor-core kernel (split pre-pass + tcgen05 GEMM)") +
                        "; per-rank M-row shard",
                    "M": M, "K": K, "N": N, "precision": args.precision,
                    "plan": {"tile_m": plan.tile_m, "tile_n": plan.tile_n, "split_k": plan.split_k},
-                   "l2": f"inputs larger than L2: A+B+C = {3 * S * S * 4 / 2**20:.0f} MiB, planes "
-                         f"{ws_bytes / 2**20:.0f} MiB > 126 MB", "parallelism": f"replicas x{world} (M-row shards)"},
+                   "l2": f"A+B+C = {4 * (M * K + K * N + M * N) / 2**20:.0f} MiB, workspace "
+                         f"{ws_bytes / 2**20:.0f} MiB (L2 126 MB)", "parallelism": f"replicas x{world} (M-row shards)"},
         "clocks": clocks,
-        "gpu_launches": (1 if prec == 0 else 3) * args.steps,
+        "gpu_launches": launches_per_step(plan, K) * args.steps,
     }
 
     if not args.no_extras:
@@ -560,7 +582,6 @@ def main() -> None:
             del mws
         out["speedup_vs_simt"] = (flops / t_step) / (flops / t_simt)
         out["speedup_vs_simt_gemm_only"] = t_simt / t_gemm
-        out["gpu_launches"] = 3 * args.steps
         # ---- FP64-measured error of both kernels (cuBLAS DGEMM as the FP64 product, outside timing)
         if rank == 0:
             with torch.no_grad():

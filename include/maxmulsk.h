@@ -91,6 +91,12 @@ enum {
     MAXMULSK_TC_REUSE_PLANES = 1,  /* the workspace already holds the planes of these
                                       A and B (a previous call with the same inputs,
                                       shape, precision and workspace): skip the split */
+    MAXMULSK_TC_FUSED_SPLIT = 2,   /* split inside the GEMM kernel: FP32 tiles of A and
+                                      B are loaded and cut into limbs on the fly, with
+                                      no planes in memory. BF16X6 / BF16X9, 128 x 128
+                                      tiles, K and N multiples of 4. Pointers that are
+                                      not 16-byte aligned run the split-inputs path
+                                      (same result), so the workspace is sized for it */
 };
 
 /* The analog of the reference's Blocking (sme/v4/sme-1x4-kcout-ncblock-apack4za.hpp:30,
@@ -103,7 +109,8 @@ enum {
  *               first slice first, like the reference's outer-Kc panels
  *               (sme/v3/sme-1x4-acc-kcout.cpp:464-471, 530-558).
  *   variant   : FP32: MAXMULSK_FP32_FMA or MAXMULSK_FP32_SCALAR.
- *               Tensor cores: MAXMULSK_TC_SPLIT_INPUTS or MAXMULSK_TC_REUSE_PLANES. */
+ *               Tensor cores: MAXMULSK_TC_SPLIT_INPUTS, MAXMULSK_TC_REUSE_PLANES or
+ *               MAXMULSK_TC_FUSED_SPLIT. */
 typedef struct {
     int32_t precision;
     int32_t tile_m;

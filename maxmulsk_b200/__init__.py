@@ -41,6 +41,7 @@ FP32_FMA = 0
 FP32_SCALAR = 1
 TC_SPLIT_INPUTS = 0
 TC_REUSE_PLANES = 1
+TC_FUSED_SPLIT = 2
 
 
 class MaxMulSKError(RuntimeError):
@@ -197,6 +198,12 @@ def slice_len(K: int, split_k: int) -> int:
     return min(per, K)
 
 
+def slice_count(K: int, split_k: int) -> int:
+    """K slices a plan actually runs (the kernels' rule, internal.hpp slice_count)."""
+    kc = slice_len(K, split_k)
+    return (K + kc - 1) // kc if kc else 1
+
+
 def stream_status(stream=None) -> Status:
     return Status(lib().maxmulsk_stream_status(_stream_ptr(stream)))
 
@@ -297,10 +304,10 @@ def _plan_with_ws(a, b, c, M, K, N, plan, stream):
 
 
 __all__ = [
-    "Status", "Precision", "Plan", "Problem", "FP32_FMA", "FP32_SCALAR", "TC_SPLIT_INPUTS", "TC_REUSE_PLANES",
+    "Status", "Precision", "Plan", "Problem", "FP32_FMA", "FP32_SCALAR", "TC_SPLIT_INPUTS", "TC_REUSE_PLANES", "TC_FUSED_SPLIT",
     "MaxMulSKError",
     "sgemm_v3", "sgemm_v4", "sgemm_plan", "sgemm_split",
     "sgemm_v3_dev", "sgemm_v4_dev", "sgemm_plan_dev", "sgemm_split_dev",
-    "make_plan", "classify", "choose", "choose_rule", "workspace_bytes", "slice_len",
+    "make_plan", "classify", "choose", "choose_rule", "workspace_bytes", "slice_len", "slice_count",
     "stream_status", "status_string", "last_error_message", "version", "check", "matmul", "lib", "Grouped",
 ]

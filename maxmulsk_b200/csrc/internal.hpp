@@ -41,6 +41,8 @@ struct SimtArgs {
     int splits;            // slices actually run (>= 1)
     float* partial;        // splits * M * N floats when splits > 1
     unsigned* counters;    // one per output tile when splits > 1 (zero on entry)
+    int reduce_after;      // set by simt_launch: slices only write partials, a
+                           // separate kernel sums them (zero everywhere else)
 };
 // Workspace bytes for the SIMT path with this tile/split choice.
 size_t simt_workspace_bytes(int64_t M, int64_t K, int64_t N, int tile_m, int tile_n, int split_k);
@@ -73,6 +75,7 @@ struct TcArgs {
     int tile_n;            // 64, 128 or 256
     int split_k;           // the plan's split_k
     bool reuse_planes;     // skip the split pre-pass: planes are already in place
+    bool fused;            // split inside the GEMM kernel (BF16 modes, 128 x 128 tiles)
     void* planes;          // operand planes written by the split pre-pass
     void* b_planes;        // B's planes split earlier (split_one as_b), or null:
                            // then they follow A's planes in `planes`

@@ -48,8 +48,14 @@ maxmulsk_status classify_plan(size_t M, size_t K, size_t N, const maxmulsk_plan*
             set_error_message("tensor-core tiles: 128x64, 128x128, 128x256 (one CTA), 256x128, 256x256 (CTA pair)");
             return MAXMULSK_ERR_UNSUPPORTED;
         }
-        if (p.variant != MAXMULSK_TC_SPLIT_INPUTS && p.variant != MAXMULSK_TC_REUSE_PLANES) {
+        if (p.variant != MAXMULSK_TC_SPLIT_INPUTS && p.variant != MAXMULSK_TC_REUSE_PLANES &&
+            p.variant != MAXMULSK_TC_FUSED_SPLIT) {
             set_error_message("unknown tensor-core variant");
+            return MAXMULSK_ERR_UNSUPPORTED;
+        }
+        if (p.variant == MAXMULSK_TC_FUSED_SPLIT &&
+            (p.precision == MAXMULSK_PREC_3XTF32 || p.tile_m != 128 || p.tile_n != 128 || K % 4 != 0 || N % 4 != 0)) {
+            set_error_message("the fused split runs BF16X6 / BF16X9 on 128x128 tiles with K and N multiples of 4");
             return MAXMULSK_ERR_UNSUPPORTED;
         }
         if (M > kMaxDim || N > kMaxDim || K > kMaxDim) { set_error_message("dimension too large"); return MAXMULSK_ERR_UNSUPPORTED; }

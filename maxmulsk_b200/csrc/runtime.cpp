@@ -157,6 +157,11 @@ maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t
     a.tile_m = plan.tile_m;
     a.tile_n = plan.tile_n;
     a.reuse_planes = (plan.variant == MAXMULSK_TC_REUSE_PLANES);
+    // The fused split loads A and B with TMA: 16-byte aligned starts (row
+    // lengths are checked by classify_plan). Otherwise the split-inputs path,
+    // whose result is the same.
+    a.fused = plan.variant == MAXMULSK_TC_FUSED_SPLIT && (reinterpret_cast<uintptr_t>(dA) & 15) == 0 &&
+              (reinterpret_cast<uintptr_t>(dB) & 15) == 0 && b_planes == nullptr;
     a.split_k = plan.split_k;
     a.err = ds->err_word;
     a.b_planes = a.reuse_planes ? nullptr : b_planes;
@@ -289,8 +294,8 @@ maxmulsk_status host_pipelined(HostStage& hs, const float* A, const float* B, fl
     st = cuda_status(cudaStreamWaitEvent(s, hs.b_in, 0), "cudaStreamWaitEvent");
     if (st != MAXMULSK_OK) return fail(st);
     void* b_planes = nullptr;
-    if (plan.precision != MAXMULSK_PREC_FP32) {
-        // B's planes once for all blocks.
+    if (plan.precision != MAXMULSK_PREC_FP32 && plan.variant != MAXMULSK_TC_FUSED_SPLIT) {
+        // B's planes once for all blocks (the fused split makes none).
         const size_t nb = split_one_bytes((int64_t)K, (int64_t)N, plan.precision, true);
         st = cuda_status(grow(&hs.dBp, &hs.capBp, (nb + sizeof(float) - 1) / sizeof(float)), "cudaMalloc(B planes)");
         if (st != MAXMULSK_OK) return fail(st);

@@ -40,9 +40,15 @@ __device__ __forceinline__ float mac(float a, float b, float c) {
 }
 
 // Shared-memory stages of one CTA.
+//
+// A is stored k-major: As[k][m ^ swz(k)]. A warp's transposing stores write
+// 8 rows for each of the k's kq, kq+4, kq+8, kq+12 of its float4 loads; with
+// rows of BM + 4 floats, k and k + 8 fall on the same banks, so rows of k >= 8
+// are stored with bit 3 of the row index flipped. Groups of four rows stay
+// contiguous and 16-byte aligned for the float4 reads of the product loop.
 template <int BM, int BN>
 struct SimtSmem {
-    float As[2][kBK][BM + 4];                       // k-major A, padded rows
+    float As[2][kBK][BM + 4];                       // k-major A, padded rows, swizzled
     float Bs[2][kBK][BN];
     int last;
 };
@@ -120,10 +126,11 @@ __device__ __forceinline__ void simt_tile(const SimtArgs& p, int64_t m0, int64_t
             const int f = tid + j * kThreads;
             const int row = f / (kBK / 4);
             const int kq = (f % (kBK / 4)) * 4;
-            As[buf][kq + 0][row] = ra[j].x;
-            As[buf][kq + 1][row] = ra[j].y;
-            As[buf][kq + 2][row] = ra[j].z;
-            As[buf][kq + 3][row] = ra[j].w;
+            const int srow = row ^ (kq & 8);
+            As[buf][kq + 0][srow] = ra[j].x;
+            As[buf][kq + 1][srow] = ra[j].y;
+            As[buf][kq + 2][srow] = ra[j].z;
+            As[buf][kq + 3][srow] = ra[j].w;
         }
 #pragma unroll
         for (int j = 0; j < B_F4; j++) {
@@ -148,23 +155,29 @@ __device__ __forceinline__ void simt_tile(const SimtArgs& p, int64_t m0, int64_t
         for (int64_t t = 0; t < ntiles; t++) {
             const int buf = (int)(t & 1);
             if (t + 1 < ntiles) load_tile(kbeg + (t + 1) * kBK);
-#pragma unroll
-            for (int k = 0; k < kBK; k++) {
-                float a[TM], b[TN];
+            // Fragments of step k + 1 are read from shared memory while the
+            // products of step k run (two register sets, fully unrolled).
+            float a[2][TM], b[2][TN];
+            auto load_frag = [&](int set, int k) {
 #pragma unroll
                 for (int g = 0; g < GM; g++) {
-                    float4 v = *reinterpret_cast<const float4*>(&As[buf][k][g * 64 + ty * 4]);
-                    a[g * 4 + 0] = v.x; a[g * 4 + 1] = v.y; a[g * 4 + 2] = v.z; a[g * 4 + 3] = v.w;
+                    float4 v = *reinterpret_cast<const float4*>(&As[buf][k][(g * 64 + ty * 4) ^ (k & 8)]);
+                    a[set][g * 4 + 0] = v.x; a[set][g * 4 + 1] = v.y; a[set][g * 4 + 2] = v.z; a[set][g * 4 + 3] = v.w;
                 }
 #pragma unroll
                 for (int g = 0; g < GN; g++) {
                     float4 v = *reinterpret_cast<const float4*>(&Bs[buf][k][g * 64 + tx * 4]);
-                    b[g * 4 + 0] = v.x; b[g * 4 + 1] = v.y; b[g * 4 + 2] = v.z; b[g * 4 + 3] = v.w;
+                    b[set][g * 4 + 0] = v.x; b[set][g * 4 + 1] = v.y; b[set][g * 4 + 2] = v.z; b[set][g * 4 + 3] = v.w;
                 }
+            };
+            load_frag(0, 0);
+#pragma unroll
+            for (int k = 0; k < kBK; k++) {
+                if (k + 1 < kBK) load_frag((k + 1) & 1, k + 1);
 #pragma unroll
                 for (int i = 0; i < TM; i++)
 #pragma unroll
-                    for (int j = 0; j < TN; j++) acc[i][j] = mac<FUSED>(a[i], b[j], acc[i][j]);
+                    for (int j = 0; j < TN; j++) acc[i][j] = mac<FUSED>(a[k & 1][i], b[k & 1][j], acc[i][j]);
             }
             if (t + 1 < ntiles) store_tile(buf ^ 1);
             __syncthreads();
@@ -217,6 +230,7 @@ __device__ __forceinline__ void simt_tile(const SimtArgs& p, int64_t m0, int64_t
                 if (c + j < N) __stcg(mine + r * N + c + j, acc[i][g * 4 + j]);
         }
     }
+    if (p.reduce_after) return;                      // summed by simt_splitk_reduce_kernel
     __threadfence();
     __syncthreads();
     if (tid == 0) {
@@ -291,8 +305,48 @@ sgemm_simt_grouped_kernel(const GroupProblem* __restrict__ probs, const GroupUni
     }
 }
 
+// Split-K reduction for plans of three or more K slices: the slices wrote
+// their partial products ([slice][M][N]); each thread sums one output (four
+// adjacent columns where rows allow 128-bit access) over the slices in slice
+// order -- the order of the in-kernel fixup and of the reference's panel sum
+// C = p0 + p1 + ... -- so C is the same bit for bit. All outputs proceed in
+// parallel, instead of one CTA per tile walking its slices in turn.
+// HBM-bound: splits * M * N floats in, M * N out.
+__global__ void __launch_bounds__(256)
+simt_splitk_reduce_kernel(const float* __restrict__ partial, float* __restrict__ C, int64_t M, int64_t N,
+                          int splits, int vec) {
+    const size_t MN = (size_t)M * (size_t)N;
+    const int64_t items = vec ? (int64_t)(MN / 4) : (int64_t)MN;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < items;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (vec) {
+            const float4* src = reinterpret_cast<const float4*>(partial) + i;
+            float4 acc = __ldcs(src);
+#pragma unroll 8
+            for (int z = 1; z < splits; z++) {
+                const float4 v = __ldcs(src + (size_t)z * (MN / 4));
+                acc.x = __fadd_rn(acc.x, v.x);
+                acc.y = __fadd_rn(acc.y, v.y);
+                acc.z = __fadd_rn(acc.z, v.z);
+                acc.w = __fadd_rn(acc.w, v.w);
+            }
+            reinterpret_cast<float4*>(C)[i] = acc;
+        } else {
+            float acc = __ldcs(partial + i);
+#pragma unroll 8
+            for (int z = 1; z < splits; z++) acc = __fadd_rn(acc, __ldcs(partial + (size_t)z * MN + i));
+            C[i] = acc;
+        }
+    }
+}
+
+// Slices at or above which the partials are summed by the reduction kernel.
+constexpr int kReduceAfterSplits = 3;
+
 template <int BM, int BN>
-cudaError_t launch_tile(const SimtArgs& a, int variant, cudaStream_t s) {
+cudaError_t launch_tile(const SimtArgs& args, int variant, cudaStream_t s) {
+    SimtArgs a = args;
+    a.reduce_after = (a.splits >= kReduceAfterSplits) ? 1 : 0;
     dim3 grid((unsigned)((a.N + BN - 1) / BN), (unsigned)((a.M + BM - 1) / BM), (unsigned)a.splits);
     const bool vec = (a.K % 4 == 0) && (a.N % 4 == 0) &&
                      ((uintptr_t)a.A % 16 == 0) && ((uintptr_t)a.B % 16 == 0) && ((uintptr_t)a.C % 16 == 0);
@@ -301,6 +355,14 @@ cudaError_t launch_tile(const SimtArgs& a, int variant, cudaStream_t s) {
     else if (fused) sgemm_simt_kernel<BM, BN, true, false><<<grid, kThreads, 0, s>>>(a);
     else if (vec) sgemm_simt_kernel<BM, BN, false, true><<<grid, kThreads, 0, s>>>(a);
     else sgemm_simt_kernel<BM, BN, false, false><<<grid, kThreads, 0, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !a.reduce_after) return e;
+    const int rvec = (a.N % 4 == 0) && ((uintptr_t)a.C % 16 == 0) && ((uintptr_t)a.partial % 16 == 0);
+    const int64_t items = rvec ? a.M * a.N / 4 : a.M * a.N;
+    int64_t blocks = (items + 255) / 256;
+    const int64_t cap = (int64_t)device_sm_count() * 8;
+    if (cap > 0 && blocks > cap) blocks = cap;
+    simt_splitk_reduce_kernel<<<(unsigned)blocks, 256, 0, s>>>(a.partial, a.C, a.M, a.N, a.splits, rvec);
     return cudaGetLastError();
 }
 

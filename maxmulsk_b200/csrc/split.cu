@@ -26,23 +26,10 @@
 #include <cstdint>
 
 #include "internal.hpp"
+#include "split_math.cuh"
 
 namespace mmsk {
 namespace {
-
-// Round to TF32 (10 explicit mantissa bits), nearest, ties away from zero:
-// add half an ulp to the magnitude bits and clear the 13 dropped bits.
-__device__ __forceinline__ float tf32_rna(float x) {
-    uint32_t b = __float_as_uint(x);
-    return __uint_as_float((b + 0x1000u) & 0xFFFFE000u);
-}
-
-// Round to BF16, nearest, ties to even; returned as the 16 stored bits.
-__device__ __forceinline__ uint16_t bf16_rne_bits(float x) {
-    uint32_t b = __float_as_uint(x);
-    return (uint16_t)((b + 0x7FFFu + ((b >> 16) & 1u)) >> 16);
-}
-__device__ __forceinline__ float bf16_bits_to_float(uint16_t h) { return __uint_as_float((uint32_t)h << 16); }
 
 // One pass over a row-major R x Cin FP32 matrix, writing P planes of R x Cout
 // (Cout >= Cin, multiple of 4; columns >= Cin are zero). Each thread handles 4
@@ -84,22 +71,13 @@ split_kernel(const float* __restrict__ src, int64_t R, int64_t Cin, int64_t Cout
             *reinterpret_cast<float4*>(p0 + off) = make_float4(hi[0], hi[1], hi[2], hi[3]);
             *reinterpret_cast<float4*>(p1 + off) = make_float4(lo[0], lo[1], lo[2], lo[3]);
         } else {
-            uint16_t l[3][4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const uint16_t a = bf16_rne_bits(x[j]);
-                const float r1 = x[j] - bf16_bits_to_float(a);
-                const uint16_t b = bf16_rne_bits(r1);
-                const float r2 = r1 - bf16_bits_to_float(b);
-                l[0][j] = a; l[1][j] = b; l[2][j] = bf16_rne_bits(r2);
-            }
+            uint2 l[3];
+            bf16_limbs2(x[0], x[1], l[0].x, l[1].x, l[2].x);
+            bf16_limbs2(x[2], x[3], l[0].y, l[1].y, l[2].y);
 #pragma unroll
             for (int p = 0; p < 3; p++) {
                 uint16_t* dst = reinterpret_cast<uint16_t*>(reinterpret_cast<char*>(planes) + (size_t)p * plane_bytes);
-                uint2 packed;
-                packed.x = (uint32_t)l[p][0] | ((uint32_t)l[p][1] << 16);
-                packed.y = (uint32_t)l[p][2] | ((uint32_t)l[p][3] << 16);
-                *reinterpret_cast<uint2*>(dst + off) = packed;
+                *reinterpret_cast<uint2*>(dst + off) = l[p];
             }
         }
     }

@@ -53,6 +53,7 @@
 
 #include "internal.hpp"
 #include "sm100.cuh"
+#include "split_math.cuh"
 
 namespace mmsk {
 int tc_slots(int precision, int tile_m, int tile_n);
@@ -121,6 +122,7 @@ struct TcParams {
     int64_t main_kchunk, tail_kchunk;
     int max_splits;
     int chunk_kb;            // stages per TMEM accumulation chunk
+    int reduce_after;        // split tiles only write partials; tc_splitk_reduce_kernel sums them
     float* C;
     float* partial;          // [split tile][slice][128 x BN], split tiles only
     unsigned* counters;      // EPI per split tile (one per epilogue warp)
@@ -171,6 +173,137 @@ __device__ __forceinline__ Unit decode_unit(const TcParams& p, int64_t u) {
     w.kend = min(p.K, w.kbeg + kc);
     tile_coords(p, t, w.tm, w.tn);
     return w;
+}
+
+// Epilogue warps of the one-CTA kernels: each TMEM chunk of a unit is drained
+// into FP32 register sums (round to nearest, chunk after chunk in k order);
+// then the unit's tile is stored, or, for a K slice, its partial tile, and the
+// last slice to arrive sums all slices in slice order (unless a separate
+// reduction kernel does that).
+template <class Cf, int BN>
+__device__ __forceinline__ void epilogue_role(const TcParams& p, uint32_t tmem_base, uint64_t* tfull_bar,
+                                              uint64_t* tempty_bar, volatile int& abort_s, int warp, int lane) {
+    constexpr int COLS = Cf::COLS;                   // columns of one epilogue thread
+    auto fail = [&]() {
+        atomicOr(p.err, kErrTimeout);
+        abort_s = 1;
+    };
+    auto kblocks = [&](const Unit& w) -> int64_t { return (w.kend - w.kbeg + Cf::BK - 1) / Cf::BK; };
+    const int ew = warp - 2;                      // epilogue warp 0 .. EPI-1
+    const int quarter = warp & 3;                 // TMEM lanes 32*quarter .. +31
+    const int cgroup = ew / 4;                    // which COLS-wide column group
+    const int64_t M = p.M, N = p.N;
+    const bool vec = (N % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) &&
+                     (p.partial == nullptr || (reinterpret_cast<uintptr_t>(p.partial) & 15) == 0);
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    float sum[COLS];
+    bool stop = false;
+    for (int64_t u = blockIdx.x; u < p.units && !stop; u += gridDim.x) {
+        const Unit w = decode_unit(p, u);
+        const int64_t nkb = kblocks(w);
+        for (int64_t kb0 = 0; kb0 < nkb; kb0 += p.chunk_kb) {
+            int bad = abort_s;
+            if (!bad && lane == 0) {
+                if (!mbar_wait_bounded(&tfull_bar[acc], acc_phase, p.timeout)) { fail(); bad = 1; }
+            }
+            bad = __shfl_sync(0xffffffffu, bad, 0);
+            if (bad) { stop = true; break; }
+            tc_fence_after();
+            const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + cgroup * COLS);
+#pragma unroll
+            for (int c = 0; c < COLS; c += Cf::LDW) {
+                uint32_t r[Cf::LDW];
+#pragma unroll
+                for (int h = 0; h < Cf::LDW; h += 32)
+                    tmem_ld_32x32b_x32(taddr + (uint32_t)(c + h), *reinterpret_cast<uint32_t(*)[32]>(&r[h]));
+                tmem_wait_ld();
+                if (kb0 == 0) {
+#pragma unroll
+                    for (int j = 0; j < Cf::LDW; j++) sum[c + j] = __uint_as_float(r[j]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < Cf::LDW; j++) sum[c + j] = __fadd_rn(sum[c + j], __uint_as_float(r[j]));
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty_bar[acc]);
+            if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+        }
+        if (stop) break;
+
+        // ---- the unit's sums are complete: store them
+        const int lrow = quarter * 32 + lane;             // row within the tile
+        const int lcol = cgroup * COLS;                   // first column within the tile
+        const int64_t row = (int64_t)w.tm * Cf::BM + lrow;
+        const int64_t col0 = (int64_t)w.tn * BN + lcol;
+        if (w.sti < 0) {
+            if (row < M) {
+                float* dst = p.C + (size_t)row * (size_t)N + (size_t)col0;
+                if (vec && col0 + COLS <= N) {
+#pragma unroll
+                    for (int j = 0; j < COLS; j += 4)
+                        *reinterpret_cast<float4*>(dst + j) = make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < COLS; j++)
+                        if (col0 + j < N) dst[j] = sum[j];
+                }
+            }
+            continue;
+        }
+        // A slice of a split tile: write the partial tile (compact, whole
+        // rows), then the last slice to arrive for this warp's rows and
+        // columns sums all slices in slice order into C.
+        constexpr size_t TILE = (size_t)Cf::BM * BN;
+        float* part = p.partial + ((size_t)w.sti * p.max_splits + w.z) * TILE + (size_t)lrow * BN + lcol;
+#pragma unroll
+        for (int j = 0; j < COLS; j += 4)
+            __stcg(reinterpret_cast<float4*>(part + j), make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]));
+        if (p.reduce_after) continue;        // summed by tc_splitk_reduce_kernel
+        __threadfence();
+        __syncwarp();
+        int last = 0;
+        unsigned* ctr = p.counters + (size_t)w.sti * Cf::EPI + ew;
+        if (lane == 0) last = (atomicAdd(ctr, 1u) == (unsigned)(w.nsplit - 1));
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last) {
+            // Every slice of this thread's row segment, in slice order,
+            // read back with 128-bit loads (its own slice included).
+            __threadfence();
+            const float* base = p.partial + (size_t)w.sti * p.max_splits * TILE + (size_t)lrow * BN + lcol;
+#pragma unroll
+            for (int j = 0; j < COLS; j += 4) {
+                const float4 t = __ldcg(reinterpret_cast<const float4*>(base + j));
+                sum[j] = t.x; sum[j + 1] = t.y; sum[j + 2] = t.z; sum[j + 3] = t.w;
+            }
+            for (int q = 1; q < w.nsplit; q++) {
+                const float* bq = base + (size_t)q * TILE;
+#pragma unroll
+                for (int j = 0; j < COLS; j += 4) {
+                    const float4 t = __ldcg(reinterpret_cast<const float4*>(bq + j));
+                    sum[j] = __fadd_rn(sum[j], t.x);
+                    sum[j + 1] = __fadd_rn(sum[j + 1], t.y);
+                    sum[j + 2] = __fadd_rn(sum[j + 2], t.z);
+                    sum[j + 3] = __fadd_rn(sum[j + 3], t.w);
+                }
+            }
+            if (row < M) {
+                float* dst = p.C + (size_t)row * (size_t)N + (size_t)col0;
+                if (vec && col0 + COLS <= N) {
+#pragma unroll
+                    for (int j = 0; j < COLS; j += 4)
+                        *reinterpret_cast<float4*>(dst + j) = make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < COLS; j++)
+                        if (col0 + j < N) dst[j] = sum[j];
+                }
+            }
+            if (lane == 0) *ctr = 0u;
+        }
+    }
 }
 
 template <int MODE, int BN>
@@ -299,120 +432,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
     } else {
         // ------------------------------------------------------------ epilogue
-        const int ew = warp - 2;                      // epilogue warp 0 .. EPI-1
-        const int quarter = warp & 3;                 // TMEM lanes 32*quarter .. +31
-        const int cgroup = ew / 4;                    // which COLS-wide column group
-        const int64_t M = p.M, N = p.N;
-        const bool vec = (N % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) &&
-                         (p.partial == nullptr || (reinterpret_cast<uintptr_t>(p.partial) & 15) == 0);
-        int acc = 0;
-        uint32_t acc_phase = 0;
-        float sum[COLS];
-        bool stop = false;
-        for (int64_t u = blockIdx.x; u < p.units && !stop; u += gridDim.x) {
-            const Unit w = decode_unit(p, u);
-            const int64_t nkb = kblocks(w);
-            for (int64_t kb0 = 0; kb0 < nkb; kb0 += p.chunk_kb) {
-                int bad = abort_s;
-                if (!bad && lane == 0) {
-                    if (!mbar_wait_bounded(&tfull_bar[acc], acc_phase, p.timeout)) { fail(); bad = 1; }
-                }
-                bad = __shfl_sync(0xffffffffu, bad, 0);
-                if (bad) { stop = true; break; }
-                tc_fence_after();
-                const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * BN + cgroup * COLS);
-#pragma unroll
-                for (int c = 0; c < COLS; c += Cf::LDW) {
-                    uint32_t r[Cf::LDW];
-#pragma unroll
-                    for (int h = 0; h < Cf::LDW; h += 32)
-                        tmem_ld_32x32b_x32(taddr + (uint32_t)(c + h), *reinterpret_cast<uint32_t(*)[32]>(&r[h]));
-                    tmem_wait_ld();
-                    if (kb0 == 0) {
-#pragma unroll
-                        for (int j = 0; j < Cf::LDW; j++) sum[c + j] = __uint_as_float(r[j]);
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < Cf::LDW; j++) sum[c + j] = __fadd_rn(sum[c + j], __uint_as_float(r[j]));
-                    }
-                }
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&tempty_bar[acc]);
-                if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
-            }
-            if (stop) break;
-
-            // ---- the unit's sums are complete: store them
-            const int lrow = quarter * 32 + lane;             // row within the tile
-            const int lcol = cgroup * COLS;                   // first column within the tile
-            const int64_t row = (int64_t)w.tm * Cf::BM + lrow;
-            const int64_t col0 = (int64_t)w.tn * BN + lcol;
-            if (w.sti < 0) {
-                if (row < M) {
-                    float* dst = p.C + (size_t)row * (size_t)N + (size_t)col0;
-                    if (vec && col0 + COLS <= N) {
-#pragma unroll
-                        for (int j = 0; j < COLS; j += 4)
-                            *reinterpret_cast<float4*>(dst + j) = make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < COLS; j++)
-                            if (col0 + j < N) dst[j] = sum[j];
-                    }
-                }
-                continue;
-            }
-            // A slice of a split tile: write the partial tile (compact, whole
-            // rows), then the last slice to arrive for this warp's rows and
-            // columns sums all slices in slice order into C.
-            constexpr size_t TILE = (size_t)Cf::BM * BN;
-            float* part = p.partial + ((size_t)w.sti * p.max_splits + w.z) * TILE + (size_t)lrow * BN + lcol;
-#pragma unroll
-            for (int j = 0; j < COLS; j += 4)
-                __stcg(reinterpret_cast<float4*>(part + j), make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]));
-            __threadfence();
-            __syncwarp();
-            int last = 0;
-            unsigned* ctr = p.counters + (size_t)w.sti * Cf::EPI + ew;
-            if (lane == 0) last = (atomicAdd(ctr, 1u) == (unsigned)(w.nsplit - 1));
-            last = __shfl_sync(0xffffffffu, last, 0);
-            if (last) {
-                // Every slice of this thread's row segment, in slice order,
-                // read back with 128-bit loads (its own slice included).
-                __threadfence();
-                const float* base = p.partial + (size_t)w.sti * p.max_splits * TILE + (size_t)lrow * BN + lcol;
-#pragma unroll
-                for (int j = 0; j < COLS; j += 4) {
-                    const float4 t = __ldcg(reinterpret_cast<const float4*>(base + j));
-                    sum[j] = t.x; sum[j + 1] = t.y; sum[j + 2] = t.z; sum[j + 3] = t.w;
-                }
-                for (int q = 1; q < w.nsplit; q++) {
-                    const float* bq = base + (size_t)q * TILE;
-#pragma unroll
-                    for (int j = 0; j < COLS; j += 4) {
-                        const float4 t = __ldcg(reinterpret_cast<const float4*>(bq + j));
-                        sum[j] = __fadd_rn(sum[j], t.x);
-                        sum[j + 1] = __fadd_rn(sum[j + 1], t.y);
-                        sum[j + 2] = __fadd_rn(sum[j + 2], t.z);
-                        sum[j + 3] = __fadd_rn(sum[j + 3], t.w);
-                    }
-                }
-                if (row < M) {
-                    float* dst = p.C + (size_t)row * (size_t)N + (size_t)col0;
-                    if (vec && col0 + COLS <= N) {
-#pragma unroll
-                        for (int j = 0; j < COLS; j += 4)
-                            *reinterpret_cast<float4*>(dst + j) = make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < COLS; j++)
-                            if (col0 + j < N) dst[j] = sum[j];
-                    }
-                }
-                if (lane == 0) *ctr = 0u;
-            }
-        }
+        epilogue_role<Cf, BN>(p, tmem_base, tfull_bar, tempty_bar, abort_s, warp, lane);
     }
 
     tc_fence_before();
@@ -669,6 +689,7 @@ tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
 #pragma unroll
             for (int j = 0; j < COLS; j += 4)
                 __stcg(reinterpret_cast<float4*>(part + j), make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]));
+            if (p.reduce_after) continue;        // summed by tc_splitk_reduce_kernel
             __threadfence();
             __syncwarp();
             int last = 0;
@@ -756,6 +777,331 @@ cudaError_t set_smem_once(Kern kern, int bytes, std::atomic<uint64_t>& done) {
     return e;
 }
 
+// ============================================================================
+// Fused-split variant (BF16x6 / BF16x9, 128 x 128 tiles). The operands are
+// split inside the kernel instead of by the pre-pass. Warp 0 loads FP32 tiles
+// of A (128 rows x 32 k) and B (32 k x 128 n, as four 32-column boxes) with
+// TMA and the 128-byte swizzle into a staging ring; four converter warps cut
+// each staged element into its three BF16 limbs (split_math.cuh, the
+// pre-pass's arithmetic) and write the limb planes into an operand ring in
+// the layouts the MMA reads -- the bytes TMA writes for the pre-pass planes:
+// A K-major with 64-byte rows and the 64-byte swizzle, B in 128-byte column
+// panels with the 128-byte swizzle. The MMA warp and the epilogue are those
+// of the one-CTA kernel, so C is the same bit for bit as with the pre-pass.
+// Each FP32 element crosses HBM once per tile that reads it instead of being
+// read, written as planes and read again: the gain where the pre-pass costs
+// as much as the products (narrow M or N).
+// ============================================================================
+template <int MODE>
+struct CfgFused {
+    static constexpr bool TF32 = false;
+    static constexpr int P = 3;                      // BF16 limb planes per operand
+    static constexpr int ES = 2;
+    static constexpr int BM = 128, BN = 128;
+    static constexpr int BK = 32;                    // k per stage: one 64-byte row of BF16
+    static constexpr int KSTEP = 16;
+    static constexpr int KSTEPS = BK / KSTEP;
+    static constexpr int A_PLANE = BM * 64;          // 8 KB per A plane
+    static constexpr int B_PLANE = BK * BN * ES;     // 8 KB per B plane: 2 panels of 32 k x 128 bytes
+    static constexpr int OP_STAGE = P * (A_PLANE + B_PLANE);
+    static constexpr int OP_STAGES = 2;
+    static constexpr int ST_A = BM * BK * 4;         // FP32 A box: 128 rows x 128 bytes
+    static constexpr int ST_BOX = BK * 32 * 4;       // FP32 B box: 32 k x 32 n
+    static constexpr int NBOX = BN / 32;
+    static constexpr int ST_STAGE = ST_A + NBOX * ST_BOX;
+    static constexpr int ST_STAGES = 3;
+    static constexpr int SMEM = OP_STAGES * OP_STAGE + ST_STAGES * ST_STAGE + 1024;
+    static constexpr int NPROD = (MODE == MAXMULSK_PREC_BF16X6) ? 6 : 9;
+    static constexpr uint32_t IDESC = make_idesc(1u, 128u, (uint32_t)BN, 1u);
+    static constexpr uint32_t TMEM_COLS = 2 * BN;
+    static constexpr int EPI = 8;                    // epilogue warps 2 .. 9
+    static constexpr int COLS = BN * 4 / EPI;
+    static constexpr int LDW = 32;
+    static constexpr int NCONV = 4;                  // converter warps 10 .. 13
+    static constexpr int THREADS = 64 + 32 * (EPI + NCONV);
+    static_assert(NCONV * 32 == BM && NCONV == NBOX, "one converter lane per A row and per B box row");
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(CfgFused<MODE>::THREADS, 1)
+tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcParams p) {
+    using Cf = CfgFused<MODE>;
+    constexpr int BN = Cf::BN;
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t st_full[Cf::ST_STAGES];
+    __shared__ __align__(8) uint64_t st_empty[Cf::ST_STAGES];
+    __shared__ __align__(8) uint64_t op_full[Cf::OP_STAGES];
+    __shared__ __align__(8) uint64_t op_empty[Cf::OP_STAGES];
+    __shared__ __align__(8) uint64_t tfull_bar[2];
+    __shared__ __align__(8) uint64_t tempty_bar[2];
+    __shared__ __align__(8) uint64_t done_bar;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* ops = smem;                                        // operand ring (1024-aligned stages)
+    uint8_t* stg = smem + Cf::OP_STAGES * Cf::OP_STAGE;         // staging ring
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    constexpr int CONV0 = 2 + Cf::EPI;                          // first converter warp
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < Cf::ST_STAGES; s++) { mbar_init(&st_full[s], 1); mbar_init(&st_empty[s], Cf::NCONV); }
+        for (int s = 0; s < Cf::OP_STAGES; s++) { mbar_init(&op_full[s], Cf::NCONV); mbar_init(&op_empty[s], 1); }
+        for (int a = 0; a < 2; a++) { mbar_init(&tfull_bar[a], 1); mbar_init(&tempty_bar[a], Cf::EPI); }
+        mbar_init(&done_bar, 1);
+        abort_s = 0;
+        fence_mbar_init();
+        fence_proxy_async();
+    }
+    if (warp == 0 && lane == 0) { prefetch_tmap(&tmA); prefetch_tmap(&tmB); }
+    if (warp == 1) { tmem_alloc(&tmem_base_s, Cf::TMEM_COLS); tmem_relinquish(); }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = tmem_base_s;
+
+    auto fail = [&]() {
+        atomicOr(p.err, kErrTimeout);
+        abort_s = 1;
+    };
+    auto kblocks = [&](const Unit& w) -> int64_t { return (w.kend - w.kbeg + Cf::BK - 1) / Cf::BK; };
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer (FP32 tiles)
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int64_t issued = 0;
+            for (int64_t u = blockIdx.x; u < p.units && !abort_s; u += gridDim.x) {
+                const Unit w = decode_unit(p, u);
+                const int64_t nkb = kblocks(w);
+                bool ok = true;
+                for (int64_t kb = 0; kb < nkb; kb++) {
+                    if (!mbar_wait_bounded(&st_empty[stage], phase ^ 1u, p.timeout)) { fail(); ok = false; break; }
+                    if (abort_s) { ok = false; break; }
+                    uint8_t* sa = stg + (size_t)stage * Cf::ST_STAGE;
+                    mbar_arrive_expect_tx(&st_full[stage], (uint32_t)Cf::ST_STAGE);
+                    const int32_t k = (int32_t)(w.kbeg + kb * Cf::BK);
+                    tma_load_2d(sa, &tmA, &st_full[stage], k, w.tm * Cf::BM);
+#pragma unroll
+                    for (int b = 0; b < Cf::NBOX; b++)
+                        tma_load_2d(sa + Cf::ST_A + b * Cf::ST_BOX, &tmB, &st_full[stage], w.tn * BN + 32 * b, k);
+                    issued++;
+                    if (++stage == Cf::ST_STAGES) { stage = 0; phase ^= 1u; }
+                }
+                if (!ok) break;
+            }
+            // No copy may still be landing in shared memory when the CTA exits.
+            const int64_t first = issued > Cf::ST_STAGES ? issued - Cf::ST_STAGES : 0;
+            for (int64_t j = first; j < issued; j++) {
+                if (!mbar_wait_bounded(&st_full[j % Cf::ST_STAGES], (uint32_t)((j / Cf::ST_STAGES) & 1), p.timeout)) {
+                    atomicOr(p.err, kErrTimeout);
+                    abort_s = 1;
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int acc = 0;
+            uint32_t acc_phase = 0;
+            bool ok = true;
+            for (int64_t u = blockIdx.x; u < p.units && ok && !abort_s; u += gridDim.x) {
+                const int64_t nkb = kblocks(decode_unit(p, u));
+                for (int64_t kb0 = 0; kb0 < nkb && ok; kb0 += p.chunk_kb) {
+                    if (!mbar_wait_bounded(&tempty_bar[acc], acc_phase ^ 1u, p.timeout)) { fail(); ok = false; break; }
+                    tc_fence_after();
+                    const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+                    const int64_t kb1 = min(nkb, kb0 + (int64_t)p.chunk_kb);
+                    for (int64_t kb = kb0; kb < kb1; kb++) {
+                        if (!mbar_wait_bounded(&op_full[stage], phase, p.timeout)) { fail(); ok = false; break; }
+                        tc_fence_after();
+                        const uint32_t a_base = smem_u32(ops + (size_t)stage * Cf::OP_STAGE);
+                        const uint32_t b_base = a_base + Cf::P * Cf::A_PLANE;
+#pragma unroll
+                        for (int ks = 0; ks < Cf::KSTEPS; ks++) {
+#pragma unroll
+                            for (int q = 0; q < Cf::NPROD; q++) {
+                                int pa, pb;
+                                product_planes(MODE, q, pa, pb);
+                                const uint64_t adesc =
+                                    make_smem_desc(a_base + (uint32_t)(pa * Cf::A_PLANE + ks * 32), 16u, 512u, 4u);
+                                const uint64_t bdesc =
+                                    make_smem_desc(b_base + (uint32_t)(pb * Cf::B_PLANE + ks * Cf::KSTEP * 128),
+                                                   (uint32_t)(Cf::BK * 128), 1024u, 2u);
+                                const uint32_t accum = (kb > kb0 || ks > 0 || q > 0) ? 1u : 0u;
+                                mma_bf16(d_tmem, adesc, bdesc, Cf::IDESC, accum);
+                            }
+                        }
+                        tc_commit(&op_empty[stage]);
+                        if (++stage == Cf::OP_STAGES) { stage = 0; phase ^= 1u; }
+                    }
+                    if (!ok) break;
+                    tc_commit(&tfull_bar[acc]);
+                    if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+                }
+            }
+            // No MMA may still be running when TMEM is freed.
+            tc_commit(&done_bar);
+            if (!mbar_wait_bounded(&done_bar, 0u, p.timeout)) { atomicOr(p.err, kErrTimeout); abort_s = 1; }
+        }
+    } else if (warp < CONV0) {
+        // ------------------------------------------------------------ epilogue
+        epilogue_role<Cf, BN>(p, tmem_base, tfull_bar, tempty_bar, abort_s, warp, lane);
+    } else {
+        // ------------------------------------------------------------ converters
+        // Warp cw splits A rows 32cw .. 32cw+31 (one per lane) and the 32 k
+        // rows of B box cw (columns 32cw .. 32cw+31), one k row per lane.
+        // Shared-memory accesses: a quarter-warp covers 8 consecutive rows,
+        // whose swizzled 16-byte chunks fall on distinct banks.
+        const int cw = warp - CONV0;
+        int stage = 0, ostage = 0;
+        uint32_t phase = 0, ophase = 0;
+        bool stop = false;
+        for (int64_t u = blockIdx.x; u < p.units && !stop; u += gridDim.x) {
+            const int64_t nkb = kblocks(decode_unit(p, u));
+            for (int64_t kb = 0; kb < nkb; kb++) {
+                int bad = abort_s;
+                if (!bad && lane == 0) {
+                    if (!mbar_wait_bounded(&op_empty[ostage], ophase ^ 1u, p.timeout) ||
+                        !mbar_wait_bounded(&st_full[stage], phase, p.timeout)) {
+                        fail();
+                        bad = 1;
+                    }
+                }
+                bad = __shfl_sync(0xffffffffu, bad, 0);
+                if (bad) { stop = true; break; }
+                const uint8_t* sa = stg + (size_t)stage * Cf::ST_STAGE;
+                uint8_t* oa = ops + (size_t)ostage * Cf::OP_STAGE;
+                {
+                    // A row r: 32 FP32 k's (128-byte row, 128-byte swizzle) ->
+                    // three 64-byte BF16 rows (64-byte swizzle).
+                    const int r = cw * 32 + lane;
+                    float x[32];
+#pragma unroll
+                    for (int c = 0; c < 8; c++) {
+                        const float4 v = *reinterpret_cast<const float4*>(sa + r * 128 + ((c ^ (r & 7)) << 4));
+                        x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        uint32_t l0[4], l1[4], l2[4];
+#pragma unroll
+                        for (int e = 0; e < 4; e++) bf16_limbs2(x[8 * j + 2 * e], x[8 * j + 2 * e + 1], l0[e], l1[e], l2[e]);
+                        const int off = r * 64 + ((j ^ ((r >> 1) & 3)) << 4);
+                        *reinterpret_cast<uint4*>(oa + off) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
+                        *reinterpret_cast<uint4*>(oa + Cf::A_PLANE + off) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
+                        *reinterpret_cast<uint4*>(oa + 2 * Cf::A_PLANE + off) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
+                    }
+                }
+                {
+                    // B row k of box cw: 32 FP32 n's -> four 16-byte chunks of
+                    // 8 BF16 in column panel cw / 2, chunks 4 (cw % 2) .. +3.
+                    const int k = lane;
+                    const uint8_t* sb = sa + Cf::ST_A + cw * Cf::ST_BOX;
+                    float x[32];
+#pragma unroll
+                    for (int c = 0; c < 8; c++) {
+                        const float4 v = *reinterpret_cast<const float4*>(sb + k * 128 + ((c ^ (k & 7)) << 4));
+                        x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
+                    }
+                    uint8_t* ob = oa + Cf::P * Cf::A_PLANE + (cw >> 1) * (Cf::BK * 128) + k * 128;
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        uint32_t l0[4], l1[4], l2[4];
+#pragma unroll
+                        for (int e = 0; e < 4; e++) bf16_limbs2(x[8 * j + 2 * e], x[8 * j + 2 * e + 1], l0[e], l1[e], l2[e]);
+                        const int off = ((((cw & 1) * 4 + j) ^ (k & 7)) << 4);
+                        *reinterpret_cast<uint4*>(ob + off) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
+                        *reinterpret_cast<uint4*>(ob + Cf::B_PLANE + off) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
+                        *reinterpret_cast<uint4*>(ob + 2 * Cf::B_PLANE + off) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
+                    }
+                }
+                // The planes are read by the tensor cores (async proxy).
+                fence_proxy_async();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&op_full[ostage]);
+                    mbar_arrive(&st_empty[stage]);
+                }
+                if (++stage == Cf::ST_STAGES) { stage = 0; phase ^= 1u; }
+                if (++ostage == Cf::OP_STAGES) { ostage = 0; ophase ^= 1u; }
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, Cf::TMEM_COLS);
+    }
+}
+
+// Split-K reduction for plans that cut every tile into K slices. The GEMM
+// wrote one partial tile per (128-row half, slice); each thread here sums one
+// float4 of a partial row over the slices in slice order -- the order of the
+// in-kernel fixup, so C is the same bit for bit -- and stores it. The slices
+// of a tile are read by many threads at once, instead of one warp walking
+// them in turn at the end of the GEMM. HBM-bound: nsplit partials in, C out.
+template <int BN>
+__global__ void __launch_bounds__(256)
+tc_splitk_reduce_kernel(const TcParams p) {
+    constexpr int Q = BN / 4;                                  // float4 per partial row
+    constexpr size_t TILE = (size_t)128 * BN;
+    const int halves = p.bm / 128;
+    const int64_t total = p.tiles * halves * 128 * Q;
+    const bool vec = (p.N % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int q4 = (int)(i % Q);
+        const int lrow = (int)((i / Q) % 128);
+        const int64_t th = i / ((int64_t)Q * 128);             // tile * halves + half
+        int tm, tn;
+        tile_coords(p, th / halves, tm, tn);
+        const int64_t row = (int64_t)tm * p.bm + (th % halves) * 128 + lrow;
+        const int64_t col = (int64_t)tn * BN + q4 * 4;
+        if (row >= p.M || col >= p.N) continue;
+        const float* src = p.partial + (size_t)th * p.max_splits * TILE + (size_t)lrow * BN + (size_t)q4 * 4;
+        float4 acc = __ldcs(reinterpret_cast<const float4*>(src));
+#pragma unroll 8
+        for (int z = 1; z < p.main_splits; z++) {
+            const float4 v = __ldcs(reinterpret_cast<const float4*>(src + (size_t)z * TILE));
+            acc.x = __fadd_rn(acc.x, v.x);
+            acc.y = __fadd_rn(acc.y, v.y);
+            acc.z = __fadd_rn(acc.z, v.z);
+            acc.w = __fadd_rn(acc.w, v.w);
+        }
+        float* dst = p.C + (size_t)row * (size_t)p.N + (size_t)col;
+        if (vec && col + 3 < p.N) {
+            *reinterpret_cast<float4*>(dst) = acc;
+        } else {
+            dst[0] = acc.x;
+            if (col + 1 < p.N) dst[1] = acc.y;
+            if (col + 2 < p.N) dst[2] = acc.z;
+            if (col + 3 < p.N) dst[3] = acc.w;
+        }
+    }
+}
+
+// A K split of every tile into at least this many slices is summed by
+// tc_splitk_reduce_kernel; fewer slices (and tail-wave splits) by the last
+// slice to arrive, inside the GEMM.
+constexpr int kReduceAfterSplits = 3;
+
+template <int BN>
+cudaError_t launch_reduce(const TcParams& prm, cudaStream_t s) {
+    const int64_t total = prm.tiles * (prm.bm / 128) * 128 * (BN / 4);
+    int64_t blocks = (total + 255) / 256;
+    const int64_t cap = (int64_t)device_sm_count() * 8;
+    if (cap > 0 && blocks > cap) blocks = cap;
+    tc_splitk_reduce_kernel<BN><<<(unsigned)blocks, 256, 0, s>>>(prm);
+    return cudaGetLastError();
+}
+
 // Host-side schedule of one launch (see TcParams).
 struct Sched {
     int bm;                          // rows per tile (128, or 256 for CTA pairs)
@@ -835,6 +1181,33 @@ size_t partial_bytes(const Sched& s, int tile_n) {
            align256((size_t)s.split_tiles * (s.bm / 128) * s.max_splits * 128 * (size_t)tile_n * sizeof(float));
 }
 
+// Kernel parameters of one launch: the problem, its schedule, and the K per
+// stage of the configuration (for the TMEM chunk length in stages).
+TcParams make_params(const TcArgs& a, const Sched& sc, int bk) {
+    TcParams prm;
+    prm.M = a.M; prm.K = a.K; prm.N = a.N;
+    prm.bm = sc.bm;
+    prm.tiles_m = (int)sc.tiles_m;
+    prm.tiles_n = (int)sc.tiles_n;
+    prm.tiles = sc.tiles;
+    prm.main_tiles = sc.main_tiles;
+    prm.main_units = sc.main_units;
+    prm.units = sc.units;
+    prm.main_splits = sc.main_splits;
+    prm.tail_splits = sc.tail_splits;
+    prm.main_kchunk = sc.main_kchunk;
+    prm.tail_kchunk = sc.tail_kchunk;
+    prm.max_splits = sc.max_splits;
+    prm.chunk_kb = chunk_len(a.K, sc.main_splits) / bk;
+    prm.reduce_after = (sc.main_splits >= kReduceAfterSplits) ? 1 : 0;
+    prm.C = a.C;
+    prm.partial = a.partial;
+    prm.counters = a.counters;
+    prm.err = a.err;
+    prm.timeout = 2000000000LL;   // about one second at B200 clocks
+    return prm;
+}
+
 template <int MODE, int BN>
 cudaError_t launch_cfg(const TcArgs& a, cudaStream_t s) {
     using Cf = Cfg<MODE, BN>;
@@ -878,33 +1251,16 @@ cudaError_t launch_cfg(const TcArgs& a, cudaStream_t s) {
     }
 
     const Sched sc = make_sched(a.M, a.K, a.N, 128, BN, a.split_k, tc_slots(a.precision, 128, BN));
-    TcParams prm;
-    prm.M = a.M; prm.K = a.K; prm.N = a.N;
-    prm.bm = 128;
-    prm.tiles_m = (int)sc.tiles_m;
-    prm.tiles_n = (int)sc.tiles_n;
-    prm.tiles = sc.tiles;
-    prm.main_tiles = sc.main_tiles;
-    prm.main_units = sc.main_units;
-    prm.units = sc.units;
-    prm.main_splits = sc.main_splits;
-    prm.tail_splits = sc.tail_splits;
-    prm.main_kchunk = sc.main_kchunk;
-    prm.tail_kchunk = sc.tail_kchunk;
-    prm.max_splits = sc.max_splits;
-    prm.chunk_kb = chunk_len(a.K, sc.main_splits) / Cf::BK;
-    prm.C = a.C;
-    prm.partial = a.partial;
-    prm.counters = a.counters;
-    prm.err = a.err;
-    prm.timeout = 2000000000LL;   // about one second at B200 clocks
+    const TcParams prm = make_params(a, sc, Cf::BK);
     if (sc.split_tiles > 0 && (!a.partial || !a.counters)) return cudaErrorInvalidValue;
 
     static std::atomic<uint64_t> smem_set{0};
     cudaError_t e = set_smem_once(tc_gemm_kernel<MODE, BN>, Cf::SMEM, smem_set);
     if (e != cudaSuccess) return e;
     tc_gemm_kernel<MODE, BN><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, prm);
-    return cudaGetLastError();
+    e = cudaGetLastError();
+    if (e != cudaSuccess || !prm.reduce_after) return e;
+    return launch_reduce<BN>(prm, s);
 }
 
 template <int MODE, int BN>
@@ -950,26 +1306,7 @@ cudaError_t launch_cfg_pair(const TcArgs& a, cudaStream_t s) {
     }
 
     const Sched sc = make_sched(a.M, a.K, a.N, 256, BN, a.split_k, tc_slots(a.precision, 256, BN));
-    TcParams prm;
-    prm.M = a.M; prm.K = a.K; prm.N = a.N;
-    prm.bm = 256;
-    prm.tiles_m = (int)sc.tiles_m;
-    prm.tiles_n = (int)sc.tiles_n;
-    prm.tiles = sc.tiles;
-    prm.main_tiles = sc.main_tiles;
-    prm.main_units = sc.main_units;
-    prm.units = sc.units;
-    prm.main_splits = sc.main_splits;
-    prm.tail_splits = sc.tail_splits;
-    prm.main_kchunk = sc.main_kchunk;
-    prm.tail_kchunk = sc.tail_kchunk;
-    prm.max_splits = sc.max_splits;
-    prm.chunk_kb = chunk_len(a.K, sc.main_splits) / Cf::BK;
-    prm.C = a.C;
-    prm.partial = a.partial;
-    prm.counters = a.counters;
-    prm.err = a.err;
-    prm.timeout = 2000000000LL;
+    const TcParams prm = make_params(a, sc, Cf::BK);
     if (sc.split_tiles > 0 && (!a.partial || !a.counters)) return cudaErrorInvalidValue;
 
     static std::atomic<uint64_t> smem_set{0};
@@ -989,7 +1326,52 @@ cudaError_t launch_cfg_pair(const TcArgs& a, cudaStream_t s) {
     cfg.numAttrs = 1;
     e = cudaLaunchKernelEx(&cfg, tc_gemm_pair_kernel<MODE, BN>, tmA, tmB, prm);
     if (e != cudaSuccess) return e;
-    return cudaGetLastError();
+    e = cudaGetLastError();
+    if (e != cudaSuccess || !prm.reduce_after) return e;
+    return launch_reduce<BN>(prm, s);
+}
+
+// The fused-split kernel reads the FP32 operands directly: A as K x M rows of
+// 4-byte elements, B as N x K; both need rows of a multiple of 16 bytes and a
+// 16-byte aligned start (checked by the caller).
+template <int MODE>
+cudaError_t launch_fused(const TcArgs& a, cudaStream_t s) {
+    using Cf = CfgFused<MODE>;
+    constexpr int BN = Cf::BN;
+    EncodeTiledFn enc = get_encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    CUtensorMap tmA, tmB;
+    {
+        const cuuint64_t dims[2] = {(cuuint64_t)a.K, (cuuint64_t)a.M};
+        const cuuint64_t strides[1] = {(cuuint64_t)a.K * 4u};
+        const cuuint32_t box[2] = {(cuuint32_t)Cf::BK, (cuuint32_t)Cf::BM};
+        const cuuint32_t estr[2] = {1, 1};
+        if (enc(&tmA, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(a.A), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return cudaErrorInvalidValue;
+    }
+    {
+        const cuuint64_t dims[2] = {(cuuint64_t)a.N, (cuuint64_t)a.K};
+        const cuuint64_t strides[1] = {(cuuint64_t)a.N * 4u};
+        const cuuint32_t box[2] = {32u, (cuuint32_t)Cf::BK};
+        const cuuint32_t estr[2] = {1, 1};
+        if (enc(&tmB, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(a.B), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return cudaErrorInvalidValue;
+    }
+    const Sched sc = make_sched(a.M, a.K, a.N, 128, BN, a.split_k, tc_slots(a.precision, 128, BN));
+    const TcParams prm = make_params(a, sc, Cf::BK);
+    if (sc.split_tiles > 0 && (!a.partial || !a.counters)) return cudaErrorInvalidValue;
+
+    static std::atomic<uint64_t> smem_set{0};
+    cudaError_t e = set_smem_once(tc_fused_kernel<MODE>, Cf::SMEM, smem_set);
+    if (e != cudaSuccess) return e;
+    tc_fused_kernel<MODE><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, prm);
+    e = cudaGetLastError();
+    if (e != cudaSuccess || !prm.reduce_after) return e;
+    return launch_reduce<BN>(prm, s);
 }
 
 template <int MODE>
@@ -1087,6 +1469,12 @@ bool tc_bind_workspace(TcArgs& a, void* ws, size_t ws_bytes) {
 }
 
 cudaError_t tc_launch(const TcArgs& a, cudaStream_t s) {
+    if (a.fused) {
+        if (a.tile_m != 128 || a.tile_n != 128) return cudaErrorInvalidValue;
+        if (a.precision == MAXMULSK_PREC_BF16X6) return launch_fused<MAXMULSK_PREC_BF16X6>(a, s);
+        if (a.precision == MAXMULSK_PREC_BF16X9) return launch_fused<MAXMULSK_PREC_BF16X9>(a, s);
+        return cudaErrorInvalidValue;
+    }
     if (!a.reuse_planes) {
         // With B's planes supplied from outside only A is split here.
         cudaError_t e = a.b_planes ? split_one(a.A, a.M, a.K, a.precision, false, a.planes, s)

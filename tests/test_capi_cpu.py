@@ -96,3 +96,15 @@ def test_probe_bytes(built_lib):
     # As B, BF16: N padded to 64 elements (128 bytes), 3 planes.
     assert built_lib.maxmulsk_probe_split_bytes(1000, 10, 2, 1) == 3 * ((1000 * 64 * 2 + 1023) // 1024 * 1024)
     assert built_lib.maxmulsk_probe_split_bytes(10, 10, 0, 1) == 0
+
+
+def test_fused_split_plan_rules(built_lib):
+    import maxmulsk_b200 as mm
+    ok = mm.make_plan(mm.Precision.BF16X6, 128, 128, 4, mm.TC_FUSED_SPLIT)
+    assert mm.classify(128, 8192, 512, ok) == mm.Status.OK
+    assert mm.classify(128, 8190, 512, ok) == mm.Status.ERR_UNSUPPORTED      # K % 4
+    assert mm.classify(128, 8192, 510, ok) == mm.Status.ERR_UNSUPPORTED      # N % 4
+    for bad in (mm.make_plan(mm.Precision.TF32X3, 128, 128, 1, mm.TC_FUSED_SPLIT),
+                mm.make_plan(mm.Precision.BF16X6, 128, 256, 1, mm.TC_FUSED_SPLIT),
+                mm.make_plan(mm.Precision.BF16X9, 256, 128, 1, mm.TC_FUSED_SPLIT)):
+        assert mm.classify(256, 256, 256, bad) == mm.Status.ERR_UNSUPPORTED

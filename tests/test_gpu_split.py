@@ -158,3 +158,39 @@ def test_split_device_entry_and_picker(cuda, oracle_mod):
     C64 = oracle_mod.dgemm(A, B, M, K, N)
     e = oracle_mod.errors(C, C64, A, B, M, K, N)
     assert e["rel_frob"] < 1e-5, e
+
+
+FUSED_SHAPES = [(128, 128, 128), (68, 68, 68), (20, 36, 40), (300, 520, 200), (256, 1024, 512), (4, 64, 4),
+                (130, 16, 300), (128, 8192, 512), (1344, 512, 2304)]
+
+
+@pytest.mark.parametrize("prec", [mm.Precision.BF16X6, mm.Precision.BF16X9])
+@pytest.mark.parametrize("split_k", [1, 2, 5])
+def test_fused_split_equals_split_inputs(cuda, oracle_mod, prec, split_k):
+    # The fused kernel splits FP32 tiles into limb planes in shared memory;
+    # the products, their order and the chunked accumulation are those of the
+    # split-inputs path on the same tiles, so C must agree bit for bit.
+    for i, (M, K, N) in enumerate(FUSED_SHAPES):
+        A = np.concatenate([oracle_mod.fill_uniform(M * K // 2, 200 + i),
+                            oracle_mod.fill_wide(M * K - M * K // 2, 300 + i)])
+        B = oracle_mod.fill_uniform(K * N, 400 + i)
+        dA, dB = to_dev(cuda, A), to_dev(cuda, B)
+        st1, C1, b1 = run_plan(cuda, A, B, M, K, N, mm.make_plan(prec, 128, 128, split_k), dA=dA, dB=dB)
+        st2, C2, b2 = run_plan(cuda, A, B, M, K, N, mm.make_plan(prec, 128, 128, split_k, mm.TC_FUSED_SPLIT),
+                               dA=dA, dB=dB)
+        assert st1 == 0 and st2 == 0, mm.last_error_message()
+        assert b1 and b2, (M, K, N)
+        assert np.array_equal(bits(C1), bits(C2)), ((M, K, N), split_k)
+
+
+def test_fused_split_unaligned_inputs_take_the_split_inputs_path(cuda, oracle_mod):
+    M, K, N = 96, 256, 128
+    A = oracle_mod.fill_uniform(M * K, 501)
+    B = oracle_mod.fill_uniform(K * N, 502)
+    Abuf = cuda.zeros(M * K + 1, device="cuda")
+    Abuf[1:] = to_dev(cuda, A)
+    plan = mm.make_plan(mm.Precision.BF16X6, 128, 128, 1, mm.TC_FUSED_SPLIT)
+    st, C, bands = run_plan(cuda, A, B, M, K, N, plan, dA=Abuf[1:])
+    assert st == 0 and bands
+    _, Cref, _ = run_plan(cuda, A, B, M, K, N, mm.make_plan(mm.Precision.BF16X6, 128, 128, 1))
+    assert np.array_equal(bits(C), bits(Cref))
