@@ -328,7 +328,7 @@ def run_tables(args) -> None:
         return
 
     # grouped batch: one persistent launch from a CUDA graph vs one launch per GEMM
-    shapes = workloads.grouped_problems()
+    shapes = workloads.grouped_problems()[: max(1, args.problems)]
     probs, keep = [], []
     for i, (M, K, N) in enumerate(shapes):
         a = torch.from_numpy(datagen.uniform(M * K, 1000 + 2 * i)).cuda()
@@ -358,12 +358,40 @@ def run_tables(args) -> None:
         fns.append(fn)
         keep.append(ws)
     t_seq = graph_time(torch, lambda: [f() for f in fns], 1)
-    emit({"workload": "grouped", "problems": len(shapes), "gflop": flops / 1e9, "units": units,
+    emit({"workload": "grouped", "precision": "fp32", "problems": len(shapes), "gflop": flops / 1e9, "units": units,
           "plan": {"tile_m": gp.tile_m, "tile_n": gp.tile_n, "split_k_max": max(splits)},
           "grouped_ms": t_group * 1e3, "grouped_gflops": flops / t_group / 1e9,
           "per_gemm_launches_ms": t_seq * 1e3, "per_gemm_launches_gflops": flops / t_seq / 1e9,
           "frac_fp32_roofline": flops / t_group / 1e12 / fp32_peak})
     g.close()
+    # split precision: the fused-split tcgen05 kernel over the group (problems
+    # with K or N not a multiple of 4 run in the FP32 part of the same graph)
+    for name, pc in (("bf16x6", 2), ("bf16x9", 3)):
+        gt = mm.Grouped(probs, mm.make_plan(pc, 128, 128, 0))
+        tp, tsplits, tunits = gt.info()
+        for _ in range(3):
+            gt.launch()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            gt.launch()
+        e1.record()
+        torch.cuda.synchronize()
+        t_tc = e0.elapsed_time(e1) / 1e3 / reps
+        peak = peaks["bf16_tflops"] / PRODUCTS[pc]
+        nw = []
+        for i in np.random.default_rng(0).choice(len(shapes), 16, replace=False):
+            a, b, c, M, K, N = probs[i]
+            ref = a.view(M, K).double() @ b.view(K, N).double()
+            nw.append(float(torch.linalg.norm(c.view(M, N).double() - ref) /
+                            (torch.linalg.norm(a.double()) * torch.linalg.norm(b.double()))))
+        emit({"workload": "grouped", "precision": name, "problems": len(shapes), "gflop": flops / 1e9,
+              "units": tunits, "fp32_fallback_problems": sum(1 for M, K, N in shapes if K % 4 or N % 4),
+              "plan": {"tile_m": 128, "tile_n": 128, "split_k_max": max(tsplits), "variant": "fused split"},
+              "grouped_ms": t_tc * 1e3, "grouped_gflops": flops / t_tc / 1e9,
+              "frac_split_roofline": flops / t_tc / 1e12 / peak,
+              "normwise_max_of_16_sampled": max(nw)})
+        gt.close()
 
 
 # ----------------------------------------------------------------------------- ours
@@ -382,6 +410,8 @@ def main() -> None:
                                                    "implies --no-extras)")
     ap.add_argument("--plan", default=None, help="precision,tile_m,tile_n,split_k instead of the picker's plan "
                                                   "(profiling runs)")
+    ap.add_argument("--problems", type=int, default=256,
+                    help="grouped workload: the first N problems of the 256-GEMM batch (profiling runs)")
     ap.add_argument("--workload", choices=["square4096", "sweep", "narrow", "grouped"], default="square4096",
                     help="square4096 (default, one JSON line) or a per-cell table of the other configurations")
     args = ap.parse_args()

@@ -23,7 +23,7 @@ LIB = os.path.join(LIBDIR, "libmaxmulsk_b200.so")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-Wall", "-I", CSRC,
+COMMON = ["-O3", "-std=c++20", "-lineinfo", "-Xcompiler", "-fPIC,-Wall", "-I", CSRC,
           "-I", os.path.join(ROOT, "include")]
 CUFLAGS = ARCH + COMMON + ["--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
 

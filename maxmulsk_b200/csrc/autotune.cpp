@@ -21,11 +21,11 @@ namespace mmsk {
 
 int candidate_plans(int cls, maxmulsk_plan* out, int cap) {
     int n = 0;
-    auto add = [&](int prec, int tm, int tn, int sk) {
+    auto add = [&](int prec, int tm, int tn, int sk, int variant = 0) {
         if (n >= cap) return;
         maxmulsk_plan p;
         std::memset(&p, 0, sizeof p);
-        p.precision = prec; p.tile_m = tm; p.tile_n = tn; p.split_k = sk;
+        p.precision = prec; p.tile_m = tm; p.tile_n = tn; p.split_k = sk; p.variant = variant;
         out[n++] = p;
     };
     if (cls == 0) {
@@ -34,12 +34,21 @@ int candidate_plans(int cls, maxmulsk_plan* out, int cap) {
         for (auto& t : tiles)
             for (int sk : splits) add(MAXMULSK_PREC_FP32, t[0], t[1], sk);
     } else {
+        // 18 + 18 planes-in-memory plans, 7 fused-split plans (narrow shapes
+        // need deep K splits), 5 narrow-tile plans: 48.
         const int modes[2] = {MAXMULSK_PREC_3XTF32, MAXMULSK_PREC_BF16X6};
-        const int tiles[4][2] = {{128, 128}, {128, 256}, {256, 256}, {128, 64}};
+        const int tiles[3][2] = {{128, 128}, {128, 256}, {256, 256}};
         const int splits[6] = {1, 2, 4, 8, 16, 32};
         for (int m : modes)
             for (auto& t : tiles)
                 for (int sk : splits) add(m, t[0], t[1], sk);
+        const int fused_splits[7] = {1, 2, 4, 8, 16, 32, 64};
+        for (int sk : fused_splits) add(MAXMULSK_PREC_BF16X6, 128, 128, sk, MAXMULSK_TC_FUSED_SPLIT);
+        add(MAXMULSK_PREC_3XTF32, 128, 64, 4);
+        add(MAXMULSK_PREC_3XTF32, 128, 64, 16);
+        add(MAXMULSK_PREC_BF16X6, 128, 64, 1);
+        add(MAXMULSK_PREC_BF16X6, 128, 64, 4);
+        add(MAXMULSK_PREC_BF16X6, 128, 64, 16);
     }
     return n;
 }

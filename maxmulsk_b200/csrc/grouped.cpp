@@ -5,10 +5,15 @@
 // .cpp:598-605): one streaming region for a list of Gemm{A, B, C, M, K, N},
 // blocking chosen per GEMM. Here the list becomes a table in device memory,
 // every GEMM is cut into (tile, K slice) units, the units are sorted heaviest
-// first, and one persistent kernel takes them from an atomic counter
-// (simt.cu, sgemm_simt_grouped_kernel). The tile shape is one per group; the
-// K split is chosen per problem so that no unit is much longer than the
-// average share of an SM.
+// first, and one persistent kernel runs them:
+//   * FP32 groups: sgemm_simt_grouped_kernel (simt.cu), units taken from an
+//     atomic counter; one tile shape per group, the K split chosen per problem
+//     so that no unit is much longer than the average share of an SM;
+//   * split-precision groups (BF16x6 / BF16x9): the fused-split tcgen05 kernel
+//     (tc.cu, tc_fused_kernel) over tables of problems, units and per-problem
+//     FP32 tensor maps, 128 x 128 tiles. A problem the fused split cannot read
+//     (K or N not a multiple of 4, A or B not 16-byte aligned) runs in the FP32
+//     grouped kernel captured in the same graph, at FP32 accuracy.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -24,6 +29,8 @@ struct maxmulsk_grouped_s {
     maxmulsk_plan plan{};
     size_t count = 0;
     std::vector<int32_t> split_k;          // per problem, as planned
+    // FP32 part
+    maxmulsk_plan simt_plan{};
     mmsk::GroupProblem* d_probs = nullptr;
     mmsk::GroupUnit* d_units = nullptr;
     int nunits = 0;
@@ -31,6 +38,13 @@ struct maxmulsk_grouped_s {
     void* d_scratch = nullptr;             // [counters of all split problems][partials]
     size_t counter_bytes = 0;
     int grid = 0;
+    // split-precision part
+    void* d_tc = nullptr;                  // [problems][units][tensor maps][counters][partials]
+    mmsk::TcGroupArgs tc{};
+    size_t tc_counter_bytes = 0;
+    void* tc_counters = nullptr;
+    int tc_grid = 0;
+    // the captured graph
     cudaStream_t cap = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -54,16 +68,208 @@ double padded_work(const maxmulsk_problem& p, int bm, int bn) {
     return (double)((p.M + bm - 1) / bm * bm) * (double)((p.N + bn - 1) / bn * bn) * (double)p.K;
 }
 
-// The tile shape with the least estimated time for the whole group.
-void pick_tile(const maxmulsk_problem* probs, size_t n, int* bm, int* bn) {
+bool runs(const maxmulsk_problem& p) { return p.M && p.N && p.K; }
+
+// The tile shape with the least estimated time for the problems `idx`.
+void pick_tile(const maxmulsk_problem* probs, const std::vector<size_t>& idx, int* bm, int* bn) {
     const int cands[3][2] = {{128, 128}, {128, 64}, {64, 64}};
     double best = -1;
     for (auto& c : cands) {
         double t = 0;
-        for (size_t i = 0; i < n; i++) t += padded_work(probs[i], c[0], c[1]);
+        for (size_t i : idx) t += padded_work(probs[i], c[0], c[1]);
         t /= tile_rate(c[0], c[1]);
         if (best < 0 || t < best) { best = t; *bm = c[0]; *bn = c[1]; }
     }
+}
+
+// K split of each problem: units no longer than a quarter of a work slot's
+// average share of the group, slices at least 256 deep, at most 64 slices.
+// fixed > 0 imposes that split on every problem.
+std::vector<int> plan_splits(const maxmulsk_problem* probs, const std::vector<size_t>& idx, int bm, int bn,
+                             int slots, int fixed) {
+    double total = 0;
+    for (size_t i : idx) total += padded_work(probs[i], bm, bn);
+    const double cap = std::max(1.0, total / (4.0 * slots));
+    std::vector<int> out(idx.size(), 1);
+    for (size_t j = 0; j < idx.size(); j++) {
+        const maxmulsk_problem& p = probs[idx[j]];
+        if (!runs(p)) continue;
+        int s = 1;
+        if (fixed > 0) {
+            s = fixed;
+        } else {
+            const double unit = (double)bm * bn * (double)p.K;
+            s = (int)std::min<double>(64.0, std::ceil(unit / cap));
+            const int kmax = (int)std::max<size_t>(1, p.K / 256);
+            s = std::max(1, std::min(s, kmax));
+        }
+        out[j] = slice_count(p.K, s) > 1 ? s : 1;
+    }
+    return out;
+}
+
+// FP32 part: the problems `idx` on the SIMT grouped kernel.
+maxmulsk_status build_simt(maxmulsk_grouped_s* g, const maxmulsk_problem* problems, const std::vector<size_t>& idx,
+                           const maxmulsk_plan& plan, int sms) {
+    const int bm = plan.tile_m, bn = plan.tile_n;
+    const std::vector<int> sk = plan_splits(problems, idx, bm, bn, 2 * sms, plan.split_k);   // 2 CTAs per SM
+    for (size_t j = 0; j < idx.size(); j++) g->split_k[idx[j]] = sk[j];
+
+    std::vector<GroupProblem> hp(idx.size());
+    std::vector<GroupUnit> hu;
+    size_t counters = 0, partials = 0;
+    std::vector<size_t> ctr_off(idx.size(), 0), part_off(idx.size(), 0);
+    for (size_t j = 0; j < idx.size(); j++) {
+        const maxmulsk_problem& p = problems[idx[j]];
+        const int splits = (p.K ? slice_count(p.K, sk[j]) : 1);
+        const size_t tiles = (size_t)((p.M + bm - 1) / bm) * ((p.N + bn - 1) / bn);
+        if (splits > 1) {
+            ctr_off[j] = counters;
+            counters += tiles * sizeof(unsigned);
+            part_off[j] = partials;
+            partials += align256((size_t)splits * p.M * p.N * sizeof(float));
+        }
+    }
+    g->counter_bytes = align256(counters);
+    const size_t scratch_bytes = g->counter_bytes + partials;
+    if (scratch_bytes) {
+        cudaError_t e = cudaMalloc(&g->d_scratch, scratch_bytes);
+        if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(grouped scratch)");
+    }
+    for (size_t j = 0; j < idx.size(); j++) {
+        const maxmulsk_problem& p = problems[idx[j]];
+        GroupProblem& q = hp[j];
+        std::memset(&q, 0, sizeof q);
+        q.a.A = p.A; q.a.B = p.B; q.a.C = p.C;
+        q.a.M = (int64_t)p.M; q.a.K = (int64_t)p.K; q.a.N = (int64_t)p.N;
+        q.a.kchunk = (int64_t)slice_len(p.K, sk[j]);
+        q.a.splits = p.K ? slice_count(p.K, sk[j]) : 1;
+        q.tiles_n = (int32_t)((p.N + bn - 1) / bn);
+        q.vec = (p.K % 4 == 0) && (p.N % 4 == 0) && ((uintptr_t)p.A % 16 == 0) && ((uintptr_t)p.B % 16 == 0) &&
+                ((uintptr_t)p.C % 16 == 0);
+        if (q.a.splits > 1) {
+            q.a.counters = reinterpret_cast<unsigned*>(static_cast<char*>(g->d_scratch) + ctr_off[j]);
+            q.a.partial = reinterpret_cast<float*>(static_cast<char*>(g->d_scratch) + g->counter_bytes + part_off[j]);
+        }
+        if (!runs(p)) continue;                               // handled by memsets
+        const int tm_n = (int)((p.M + bm - 1) / bm), tn_n = q.tiles_n;
+        for (int z = 0; z < q.a.splits; z++)
+            for (int tm = 0; tm < tm_n; tm++)
+                for (int tn = 0; tn < tn_n; tn++) hu.push_back(GroupUnit{(int32_t)j, tm, tn, z});
+    }
+    // Heaviest units first (K slice length), stable so slices stay grouped.
+    std::stable_sort(hu.begin(), hu.end(), [&](const GroupUnit& x, const GroupUnit& y) {
+        const GroupProblem& a = hp[x.problem];
+        const GroupProblem& b = hp[y.problem];
+        const int64_t la = std::min(a.a.kchunk, a.a.K - (int64_t)x.z * a.a.kchunk);
+        const int64_t lb = std::min(b.a.kchunk, b.a.K - (int64_t)y.z * b.a.kchunk);
+        return la > lb;
+    });
+    g->nunits = (int)hu.size();
+    g->grid = std::max(1, std::min(g->nunits, 2 * sms));
+    cudaError_t e;
+    if ((e = cudaMalloc(&g->d_probs, std::max<size_t>(1, idx.size()) * sizeof(GroupProblem))) != cudaSuccess ||
+        (e = cudaMalloc(&g->d_units, std::max<size_t>(1, hu.size()) * sizeof(GroupUnit))) != cudaSuccess ||
+        (e = cudaMalloc(&g->d_next, sizeof(unsigned))) != cudaSuccess)
+        return cuda_status(e, "cudaMalloc(grouped tables)");
+    if (!idx.empty() && (e = cudaMemcpy(g->d_probs, hp.data(), idx.size() * sizeof(GroupProblem),
+                                        cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cuda_status(e, "upload grouped problems");
+    if (!hu.empty() && (e = cudaMemcpy(g->d_units, hu.data(), hu.size() * sizeof(GroupUnit),
+                                       cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cuda_status(e, "upload grouped units");
+    if (g->d_scratch && g->counter_bytes) cudaMemset(g->d_scratch, 0, g->counter_bytes);
+    return MAXMULSK_OK;
+}
+
+// Split-precision part: the problems `idx` on the fused-split tcgen05 kernel.
+maxmulsk_status build_tc(maxmulsk_grouped_s* g, const maxmulsk_problem* problems, const std::vector<size_t>& idx,
+                         int precision, int fixed_split, int sms) {
+    constexpr int T = 128;                                    // tile rows and columns
+    const std::vector<int> sk = plan_splits(problems, idx, T, T, sms, fixed_split);   // 1 CTA per SM
+    const size_t n = idx.size();
+    std::vector<TcGroupProblem> hp(n);
+    std::vector<TcGroupUnit> hu;
+    std::vector<unsigned char> maps(256 * std::max<size_t>(1, n));
+    size_t counters = 0, partials = 0;
+    std::vector<size_t> ctr_off(n, 0), part_off(n, 0);
+    for (size_t j = 0; j < n; j++) {
+        const maxmulsk_problem& p = problems[idx[j]];
+        g->split_k[idx[j]] = sk[j];
+        const int splits = slice_count(p.K, sk[j]);
+        const int64_t tiles = (int64_t)((p.M + T - 1) / T) * (int64_t)((p.N + T - 1) / T);
+        if (splits > 1) {
+            ctr_off[j] = counters;
+            counters += (size_t)tiles * kTcGroupCountersPerTile * sizeof(unsigned);
+            part_off[j] = partials;
+            partials += align256(tc_group_partial_floats(tiles, splits) * sizeof(float));
+        }
+        if (!tc_fused_maps(p.A, p.B, (int64_t)p.M, (int64_t)p.K, (int64_t)p.N, &maps[256 * j])) {
+            set_error_message("grouped: tensor map encoding failed");
+            return MAXMULSK_ERR_CUDA;
+        }
+    }
+    const size_t probs_b = align256(std::max<size_t>(1, n) * sizeof(TcGroupProblem));
+    // units are counted below; reserve after building them
+    g->tc_counter_bytes = align256(counters);
+    for (size_t j = 0; j < n; j++) {
+        const maxmulsk_problem& p = problems[idx[j]];
+        TcGroupProblem& q = hp[j];
+        std::memset(&q, 0, sizeof q);
+        q.M = (int64_t)p.M; q.K = (int64_t)p.K; q.N = (int64_t)p.N;
+        q.C = p.C;
+        q.splits = slice_count(p.K, sk[j]);
+        q.kchunk = (int64_t)slice_len(p.K, sk[j]);
+        q.tiles_n = (int32_t)((p.N + T - 1) / T);
+        q.chunk_kb = tc_chunk_len((int64_t)p.K, q.splits) / 32;
+        const int tm_n = (int)((p.M + T - 1) / T);
+        for (int z = 0; z < q.splits; z++)
+            for (int tm = 0; tm < tm_n; tm++)
+                for (int tn = 0; tn < q.tiles_n; tn++) hu.push_back(TcGroupUnit{(int32_t)j, tm, tn, z});
+    }
+    std::stable_sort(hu.begin(), hu.end(), [&](const TcGroupUnit& x, const TcGroupUnit& y) {
+        const TcGroupProblem& a = hp[x.problem];
+        const TcGroupProblem& b = hp[y.problem];
+        const int64_t la = std::min(a.kchunk, a.K - (int64_t)x.z * a.kchunk);
+        const int64_t lb = std::min(b.kchunk, b.K - (int64_t)y.z * b.kchunk);
+        return la > lb;
+    });
+    const size_t units_b = align256(std::max<size_t>(1, hu.size()) * sizeof(TcGroupUnit));
+    const size_t maps_b = align256(maps.size());
+    const size_t total = probs_b + units_b + maps_b + g->tc_counter_bytes + partials;
+    cudaError_t e = cudaMalloc(&g->d_tc, total);
+    if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(grouped tensor-core tables)");
+    char* base = static_cast<char*>(g->d_tc);
+    char* d_probs = base;
+    char* d_units = d_probs + probs_b;
+    char* d_maps = d_units + units_b;
+    char* d_ctr = d_maps + maps_b;
+    char* d_part = d_ctr + g->tc_counter_bytes;
+    for (size_t j = 0; j < n; j++) {
+        if (hp[j].splits > 1) {
+            hp[j].counters = reinterpret_cast<unsigned*>(d_ctr + ctr_off[j]);
+            hp[j].partial = reinterpret_cast<float*>(d_part + part_off[j]);
+        }
+    }
+    if ((e = cudaMemcpy(d_probs, hp.data(), n * sizeof(TcGroupProblem), cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (!hu.empty() && (e = cudaMemcpy(d_units, hu.data(), hu.size() * sizeof(TcGroupUnit),
+                                        cudaMemcpyHostToDevice)) != cudaSuccess) ||
+        (e = cudaMemcpy(d_maps, maps.data(), 256 * n, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return cuda_status(e, "upload grouped tensor-core tables");
+    g->tc_counters = d_ctr;
+    g->tc.probs = reinterpret_cast<const TcGroupProblem*>(d_probs);
+    g->tc.units = reinterpret_cast<const TcGroupUnit*>(d_units);
+    g->tc.maps = d_maps;
+    g->tc.nunits = (int64_t)hu.size();
+    g->tc.err = device_error_word();
+    g->tc.timeout = 2000000000LL;                             // about one second at B200 clocks
+    g->tc_grid = (int)std::max<int64_t>(1, std::min<int64_t>(g->tc.nunits, sms));
+    if (!g->tc.err) { set_error_message("device error word unavailable"); return MAXMULSK_ERR_ALLOC; }
+    return MAXMULSK_OK;
+}
+
+bool fused_readable(const maxmulsk_problem& p) {
+    return p.K % 4 == 0 && p.N % 4 == 0 && ((uintptr_t)p.A % 16) == 0 && ((uintptr_t)p.B % 16) == 0;
 }
 
 }  // namespace
@@ -92,128 +298,74 @@ maxmulsk_status maxmulsk_grouped_create(const maxmulsk_problem* problems, size_t
     maxmulsk_plan plan;
     std::memset(&plan, 0, sizeof plan);
     plan.precision = MAXMULSK_PREC_FP32;
+    int tc_precision = 0;
     if (group_plan) {
         plan = *group_plan;
-        maxmulsk_plan probe = plan;
-        if (probe.split_k == 0) probe.split_k = 1;            // 0 = per problem, picked here
-        maxmulsk_status st = classify_plan(1, 1, 1, &probe);
-        if (st != MAXMULSK_OK) return st;
-        if (plan.precision != MAXMULSK_PREC_FP32) {
-            set_error_message("grouped launches run FP32 plans");
+        if (plan.precision == MAXMULSK_PREC_SPLIT_AUTO) plan.precision = MAXMULSK_PREC_BF16X6;
+        if (plan.precision == MAXMULSK_PREC_BF16X6 || plan.precision == MAXMULSK_PREC_BF16X9) {
+            tc_precision = plan.precision;
+            plan.tile_m = 128; plan.tile_n = 128; plan.variant = MAXMULSK_TC_FUSED_SPLIT;
+            if (plan.split_k < 0 || plan.split_k > 64) {
+                set_error_message("split_k must be 0 (per problem) or 1..64");
+                return MAXMULSK_ERR_UNSUPPORTED;
+            }
+        } else if (plan.precision != MAXMULSK_PREC_FP32) {
+            set_error_message("grouped launches run FP32, BF16X6 or BF16X9 plans");
             return MAXMULSK_ERR_UNSUPPORTED;
+        } else {
+            maxmulsk_plan probe = plan;
+            if (probe.split_k == 0) probe.split_k = 1;        // 0 = per problem, picked here
+            maxmulsk_status st = classify_plan(1, 1, 1, &probe);
+            if (st != MAXMULSK_OK) return st;
         }
-    } else {
-        pick_tile(problems, count, &plan.tile_m, &plan.tile_n);
-        plan.split_k = 0;
     }
-    const int bm = plan.tile_m, bn = plan.tile_n;
 
     std::unique_ptr<maxmulsk_grouped_s> g(new (std::nothrow) maxmulsk_grouped_s());
     if (!g) return MAXMULSK_ERR_ALLOC;
     cudaGetDevice(&g->device);
-    g->plan = plan;
     g->count = count;
     g->split_k.assign(count, 1);
     const int sms = device_sm_count() > 0 ? device_sm_count() : 148;
 
-    // Per-problem K split: units no longer than a quarter of an SM's average
-    // share of the group, slices at least 256 deep.
-    double total = 0;
-    for (size_t i = 0; i < count; i++) total += padded_work(problems[i], bm, bn);
-    const double cap = std::max(1.0, total / (4.0 * 2.0 * sms));      // 2 CTAs per SM
+    std::vector<size_t> simt_idx, tc_idx;
     for (size_t i = 0; i < count; i++) {
-        const maxmulsk_problem& p = problems[i];
-        if (!p.M || !p.N || !p.K) continue;
-        int s = 1;
-        if (plan.split_k > 0) {
-            s = plan.split_k;
-        } else {
-            const double unit = (double)bm * bn * (double)p.K;
-            s = (int)std::min<double>(64.0, std::ceil(unit / cap));
-            const int kmax = (int)std::max<size_t>(1, p.K / 256);
-            s = std::max(1, std::min(s, kmax));
-        }
-        g->split_k[i] = slice_count(p.K, s) > 1 ? s : 1;
+        if (tc_precision && runs(problems[i]) && fused_readable(problems[i])) tc_idx.push_back(i);
+        else simt_idx.push_back(i);
     }
+    maxmulsk_plan simt_plan = plan;
+    if (tc_precision || !group_plan) {
+        simt_plan.precision = MAXMULSK_PREC_FP32;
+        simt_plan.variant = MAXMULSK_FP32_FMA;
+        simt_plan.split_k = tc_precision ? 0 : plan.split_k;
+        pick_tile(problems, simt_idx, &simt_plan.tile_m, &simt_plan.tile_n);
+    }
+    if (!tc_precision) plan = simt_plan;
+    g->plan = plan;
+    g->simt_plan = simt_plan;
 
-    // Tables, scratch layout and units.
-    std::vector<GroupProblem> hp(count);
-    std::vector<GroupUnit> hu;
-    size_t counters = 0, partials = 0;
-    std::vector<size_t> ctr_off(count, 0), part_off(count, 0);
-    for (size_t i = 0; i < count; i++) {
-        const maxmulsk_problem& p = problems[i];
-        const int splits = (p.K ? slice_count(p.K, g->split_k[i]) : 1);
-        const size_t tiles = (size_t)((p.M + bm - 1) / bm) * ((p.N + bn - 1) / bn);
-        if (splits > 1) {
-            ctr_off[i] = counters;
-            counters += tiles * sizeof(unsigned);
-            part_off[i] = partials;
-            partials += align256((size_t)splits * p.M * p.N * sizeof(float));
-        }
-    }
-    g->counter_bytes = align256(counters);
-    const size_t scratch_bytes = g->counter_bytes + partials;
-    if (scratch_bytes) {
-        cudaError_t e = cudaMalloc(&g->d_scratch, scratch_bytes);
-        if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(grouped scratch)");
-    }
-    for (size_t i = 0; i < count; i++) {
-        const maxmulsk_problem& p = problems[i];
-        GroupProblem& q = hp[i];
-        std::memset(&q, 0, sizeof q);
-        q.a.A = p.A; q.a.B = p.B; q.a.C = p.C;
-        q.a.M = (int64_t)p.M; q.a.K = (int64_t)p.K; q.a.N = (int64_t)p.N;
-        q.a.kchunk = (int64_t)slice_len(p.K, g->split_k[i]);
-        q.a.splits = p.K ? slice_count(p.K, g->split_k[i]) : 1;
-        q.tiles_n = (int32_t)((p.N + bn - 1) / bn);
-        q.vec = (p.K % 4 == 0) && (p.N % 4 == 0) && ((uintptr_t)p.A % 16 == 0) && ((uintptr_t)p.B % 16 == 0) &&
-                ((uintptr_t)p.C % 16 == 0);
-        if (q.a.splits > 1) {
-            q.a.counters = reinterpret_cast<unsigned*>(static_cast<char*>(g->d_scratch) + ctr_off[i]);
-            q.a.partial = reinterpret_cast<float*>(static_cast<char*>(g->d_scratch) + g->counter_bytes + part_off[i]);
-        }
-        if (!p.M || !p.N || !p.K) continue;                   // handled by memsets below
-        const int tm_n = (int)((p.M + bm - 1) / bm), tn_n = q.tiles_n;
-        for (int z = 0; z < q.a.splits; z++)
-            for (int tm = 0; tm < tm_n; tm++)
-                for (int tn = 0; tn < tn_n; tn++) hu.push_back(GroupUnit{(int32_t)i, tm, tn, z});
-    }
-    // Heaviest units first (K slice length), stable so slices stay grouped.
-    std::stable_sort(hu.begin(), hu.end(), [&](const GroupUnit& x, const GroupUnit& y) {
-        const GroupProblem& a = hp[x.problem];
-        const GroupProblem& b = hp[y.problem];
-        const int64_t la = std::min(a.a.kchunk, a.a.K - (int64_t)x.z * a.a.kchunk);
-        const int64_t lb = std::min(b.a.kchunk, b.a.K - (int64_t)y.z * b.a.kchunk);
-        return la > lb;
-    });
-    g->nunits = (int)hu.size();
-    g->grid = std::max(1, std::min(g->nunits, 2 * sms));
-
-    cudaError_t e;
-    if ((e = cudaMalloc(&g->d_probs, std::max<size_t>(1, count) * sizeof(GroupProblem))) != cudaSuccess ||
-        (e = cudaMalloc(&g->d_units, std::max<size_t>(1, hu.size()) * sizeof(GroupUnit))) != cudaSuccess ||
-        (e = cudaMalloc(&g->d_next, sizeof(unsigned))) != cudaSuccess) {
-        maxmulsk_grouped_destroy(g.release());
-        return cuda_status(e, "cudaMalloc(grouped tables)");
-    }
-    if (count) cudaMemcpy(g->d_probs, hp.data(), count * sizeof(GroupProblem), cudaMemcpyHostToDevice);
-    if (!hu.empty()) cudaMemcpy(g->d_units, hu.data(), hu.size() * sizeof(GroupUnit), cudaMemcpyHostToDevice);
-    if (g->d_scratch && g->counter_bytes) cudaMemset(g->d_scratch, 0, g->counter_bytes);
+    maxmulsk_status st = build_simt(g.get(), problems, simt_idx, simt_plan, sms);
+    if (st == MAXMULSK_OK && !tc_idx.empty()) st = build_tc(g.get(), problems, tc_idx, tc_precision, plan.split_k, sms);
+    if (st != MAXMULSK_OK) { maxmulsk_grouped_destroy(g.release()); return st; }
 
     // Capture: K == 0 problems are zero-filled; the unit counter and the
-    // split-K arrival counters are reset; then the one persistent kernel.
-    e = cudaStreamCreateWithFlags(&g->cap, cudaStreamNonBlocking);
+    // split-K arrival counters are reset; then the persistent kernel(s).
+    cudaError_t e = cudaStreamCreateWithFlags(&g->cap, cudaStreamNonBlocking);
     if (e != cudaSuccess) { maxmulsk_grouped_destroy(g.release()); return cuda_status(e, "cudaStreamCreate"); }
     e = cudaStreamBeginCapture(g->cap, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
         for (size_t i = 0; i < count; i++)
             if (problems[i].M && problems[i].N && !problems[i].K)
                 cudaMemsetAsync(problems[i].C, 0, problems[i].M * problems[i].N * sizeof(float), g->cap);
+        if (g->tc_counters && g->tc_counter_bytes) cudaMemsetAsync(g->tc_counters, 0, g->tc_counter_bytes, g->cap);
+        if (g->tc.nunits > 0) {
+            cudaError_t el = tc_grouped_launch(g->tc, tc_precision, g->tc_grid, g->cap);
+            if (el != cudaSuccess) e = el;
+        }
         cudaMemsetAsync(g->d_next, 0, sizeof(unsigned), g->cap);
         if (g->d_scratch && g->counter_bytes) cudaMemsetAsync(g->d_scratch, 0, g->counter_bytes, g->cap);
         if (g->nunits > 0)
-            simt_grouped_launch(g->d_probs, g->d_units, g->nunits, g->d_next, bm, bn, plan.variant, g->grid, g->cap);
+            simt_grouped_launch(g->d_probs, g->d_units, g->nunits, g->d_next, simt_plan.tile_m, simt_plan.tile_n,
+                                simt_plan.variant, g->grid, g->cap);
         cudaError_t e2 = cudaStreamEndCapture(g->cap, &g->graph);
         if (e == cudaSuccess) e = e2;
     }
@@ -236,7 +388,7 @@ maxmulsk_status maxmulsk_grouped_info(maxmulsk_grouped g, maxmulsk_plan* group_p
     if (!g) return MAXMULSK_ERR_INVALID;
     if (group_plan) *group_plan = g->plan;
     if (split_k) std::memcpy(split_k, g->split_k.data(), g->count * sizeof(int32_t));
-    if (units) *units = (size_t)g->nunits;
+    if (units) *units = (size_t)g->nunits + (size_t)g->tc.nunits;
     return MAXMULSK_OK;
 }
 
@@ -249,6 +401,7 @@ void maxmulsk_grouped_destroy(maxmulsk_grouped g) {
     cudaFree(g->d_units);
     cudaFree(g->d_next);
     cudaFree(g->d_scratch);
+    cudaFree(g->d_tc);
     delete g;
 }
 

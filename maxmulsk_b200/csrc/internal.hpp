@@ -91,6 +91,40 @@ int tc_slots(int precision, int tile_m, int tile_n);
 bool tc_bind_workspace(TcArgs& a, void* ws, size_t ws_bytes);
 cudaError_t tc_launch(const TcArgs& a, cudaStream_t s);
 
+// Grouped split-precision launch (fused split kernel over many GEMMs).
+struct TcGroupProblem {
+    int64_t M, K, N;
+    float* C;
+    float* partial;        // split problems: [tile][slice][128 x 128] floats
+    unsigned* counters;    // split problems: 8 per tile (zero on entry)
+    int64_t kchunk;        // K slice length
+    int32_t tiles_n;       // tiles along N
+    int32_t splits;        // K slices (1 = whole)
+    int32_t chunk_kb;      // stages per TMEM accumulation chunk
+    int32_t pad;
+};
+struct TcGroupUnit {
+    int32_t problem, tm, tn, z;
+};
+struct TcGroupArgs {
+    const TcGroupProblem* probs;
+    const TcGroupUnit* units;
+    const void* maps;      // per problem two 128-byte CUtensorMaps: FP32 A, then FP32 B
+    int64_t nunits;
+    int* err;
+    long long timeout;
+};
+// Encodes the two FP32 tensor maps the fused split reads for one problem
+// (A: K-contiguous rows, B: N-contiguous rows) into out[0..255]. K and N
+// multiples of 4, A and B 16-byte aligned.
+bool tc_fused_maps(const float* A, const float* B, int64_t M, int64_t K, int64_t N, void* out);
+// Chunk length (k's per TMEM accumulation) the kernels use for K and a K split.
+int tc_chunk_len(int64_t K, int splits);
+cudaError_t tc_grouped_launch(const TcGroupArgs& g, int precision, int grid, cudaStream_t s);
+// Bytes of the partial tiles / counters of one split problem of a grouped launch.
+inline size_t tc_group_partial_floats(int64_t tiles, int splits) { return (size_t)tiles * splits * 128 * 128; }
+constexpr int kTcGroupCountersPerTile = 8;
+
 // Operand plane geometry. A planes are [P][M][Kp] (K-major). B planes are
 // K-major [P][N][Kp] for TF32, N-major 128-byte panels [P][Np/NBE][K][NBE]
 // for BF16. Kp pads K-major rows to 16 bytes, Np pads N to whole panels;

@@ -76,6 +76,11 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, uint64_
         :: "r"(smem_u32(dst)), "l"(tmap), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
         : "memory");
 }
+// A tensor map that lives in global memory (written by a copy, not passed as
+// a kernel parameter): make its current contents visible to the TMA unit.
+__device__ __forceinline__ void tmap_acquire(const void* tmap) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" :: "l"(tmap) : "memory");
+}
 __device__ __forceinline__ void prefetch_tmap(const void* tmap) {
     asm volatile("prefetch.tensormap [%0];" :: "l"(tmap) : "memory");
 }

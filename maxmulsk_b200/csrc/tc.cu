@@ -175,37 +175,71 @@ __device__ __forceinline__ Unit decode_unit(const TcParams& p, int64_t u) {
     return w;
 }
 
+// What the roles of a persistent kernel need to know about one work unit:
+// its tile and K slice, and the problem it belongs to.
+struct UnitView {
+    Unit w;
+    int problem;             // index in a grouped launch (0 for one GEMM)
+    int64_t M, N;
+    float* C;
+    float* partial;          // the problem's partial tiles: [split tile][slice][128 x BN]
+    unsigned* counters;      // the problem's arrival counters: EPI per split tile
+    int max_splits;          // slices per split tile in the partial layout
+    int chunk_kb;            // stages per TMEM accumulation chunk
+    int reduce_after;        // partials are summed by tc_splitk_reduce_kernel
+};
+
+// Units of one GEMM (the schedule in TcParams).
+struct SingleSrc {
+    const TcParams& p;
+    __device__ __forceinline__ int64_t units() const { return p.units; }
+    // The r-th unit of this CTA: units are dealt round-robin.
+    __device__ __forceinline__ int64_t unit_of(int64_t r) const { return r * gridDim.x + blockIdx.x; }
+    __device__ __forceinline__ void get(int64_t u, UnitView& v) const {
+        v.w = decode_unit(p, u);
+        v.problem = 0;
+        v.M = p.M; v.N = p.N; v.C = p.C; v.partial = p.partial; v.counters = p.counters;
+        v.max_splits = p.max_splits; v.chunk_kb = p.chunk_kb; v.reduce_after = p.reduce_after;
+    }
+    __device__ __forceinline__ const void* map_a(const UnitView&, const void* single) const { return single; }
+    __device__ __forceinline__ const void* map_b(const UnitView&, const void* single) const { return single; }
+    __device__ __forceinline__ void acquire(const void*, const void*) const {}
+};
+
 // Epilogue warps of the one-CTA kernels: each TMEM chunk of a unit is drained
 // into FP32 register sums (round to nearest, chunk after chunk in k order);
 // then the unit's tile is stored, or, for a K slice, its partial tile, and the
 // last slice to arrive sums all slices in slice order (unless a separate
 // reduction kernel does that).
-template <class Cf, int BN>
-__device__ __forceinline__ void epilogue_role(const TcParams& p, uint32_t tmem_base, uint64_t* tfull_bar,
-                                              uint64_t* tempty_bar, volatile int& abort_s, int warp, int lane) {
+template <class Cf, int BN, class Src>
+__device__ __forceinline__ void epilogue_role(const Src& src, int* err, long long timeout, uint32_t tmem_base,
+                                              uint64_t* tfull_bar, uint64_t* tempty_bar, volatile int& abort_s,
+                                              int warp, int lane) {
     constexpr int COLS = Cf::COLS;                   // columns of one epilogue thread
     auto fail = [&]() {
-        atomicOr(p.err, kErrTimeout);
+        atomicOr(err, kErrTimeout);
         abort_s = 1;
     };
     auto kblocks = [&](const Unit& w) -> int64_t { return (w.kend - w.kbeg + Cf::BK - 1) / Cf::BK; };
     const int ew = warp - 2;                      // epilogue warp 0 .. EPI-1
     const int quarter = warp & 3;                 // TMEM lanes 32*quarter .. +31
     const int cgroup = ew / 4;                    // which COLS-wide column group
-    const int64_t M = p.M, N = p.N;
-    const bool vec = (N % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0) &&
-                     (p.partial == nullptr || (reinterpret_cast<uintptr_t>(p.partial) & 15) == 0);
     int acc = 0;
     uint32_t acc_phase = 0;
     float sum[COLS];
     bool stop = false;
-    for (int64_t u = blockIdx.x; u < p.units && !stop; u += gridDim.x) {
-        const Unit w = decode_unit(p, u);
+    for (int64_t round = 0, u = src.unit_of(0); u < src.units() && !stop; u = src.unit_of(++round)) {
+        UnitView v;
+        src.get(u, v);
+        const Unit& w = v.w;
+        const int64_t M = v.M, N = v.N;
+        const bool vec = (N % 4 == 0) && ((reinterpret_cast<uintptr_t>(v.C) & 15) == 0) &&
+                         (v.partial == nullptr || (reinterpret_cast<uintptr_t>(v.partial) & 15) == 0);
         const int64_t nkb = kblocks(w);
-        for (int64_t kb0 = 0; kb0 < nkb; kb0 += p.chunk_kb) {
+        for (int64_t kb0 = 0; kb0 < nkb; kb0 += v.chunk_kb) {
             int bad = abort_s;
             if (!bad && lane == 0) {
-                if (!mbar_wait_bounded(&tfull_bar[acc], acc_phase, p.timeout)) { fail(); bad = 1; }
+                if (!mbar_wait_bounded(&tfull_bar[acc], acc_phase, timeout)) { fail(); bad = 1; }
             }
             bad = __shfl_sync(0xffffffffu, bad, 0);
             if (bad) { stop = true; break; }
@@ -240,7 +274,7 @@ __device__ __forceinline__ void epilogue_role(const TcParams& p, uint32_t tmem_b
         const int64_t col0 = (int64_t)w.tn * BN + lcol;
         if (w.sti < 0) {
             if (row < M) {
-                float* dst = p.C + (size_t)row * (size_t)N + (size_t)col0;
+                float* dst = v.C + (size_t)row * (size_t)N + (size_t)col0;
                 if (vec && col0 + COLS <= N) {
 #pragma unroll
                     for (int j = 0; j < COLS; j += 4)
@@ -257,22 +291,22 @@ __device__ __forceinline__ void epilogue_role(const TcParams& p, uint32_t tmem_b
         // rows), then the last slice to arrive for this warp's rows and
         // columns sums all slices in slice order into C.
         constexpr size_t TILE = (size_t)Cf::BM * BN;
-        float* part = p.partial + ((size_t)w.sti * p.max_splits + w.z) * TILE + (size_t)lrow * BN + lcol;
+        float* part = v.partial + ((size_t)w.sti * v.max_splits + w.z) * TILE + (size_t)lrow * BN + lcol;
 #pragma unroll
         for (int j = 0; j < COLS; j += 4)
             __stcg(reinterpret_cast<float4*>(part + j), make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]));
-        if (p.reduce_after) continue;        // summed by tc_splitk_reduce_kernel
+        if (v.reduce_after) continue;        // summed by tc_splitk_reduce_kernel
         __threadfence();
         __syncwarp();
         int last = 0;
-        unsigned* ctr = p.counters + (size_t)w.sti * Cf::EPI + ew;
+        unsigned* ctr = v.counters + (size_t)w.sti * Cf::EPI + ew;
         if (lane == 0) last = (atomicAdd(ctr, 1u) == (unsigned)(w.nsplit - 1));
         last = __shfl_sync(0xffffffffu, last, 0);
         if (last) {
             // Every slice of this thread's row segment, in slice order,
             // read back with 128-bit loads (its own slice included).
             __threadfence();
-            const float* base = p.partial + (size_t)w.sti * p.max_splits * TILE + (size_t)lrow * BN + lcol;
+            const float* base = v.partial + (size_t)w.sti * v.max_splits * TILE + (size_t)lrow * BN + lcol;
 #pragma unroll
             for (int j = 0; j < COLS; j += 4) {
                 const float4 t = __ldcg(reinterpret_cast<const float4*>(base + j));
@@ -290,7 +324,7 @@ __device__ __forceinline__ void epilogue_role(const TcParams& p, uint32_t tmem_b
                 }
             }
             if (row < M) {
-                float* dst = p.C + (size_t)row * (size_t)N + (size_t)col0;
+                float* dst = v.C + (size_t)row * (size_t)N + (size_t)col0;
                 if (vec && col0 + COLS <= N) {
 #pragma unroll
                     for (int j = 0; j < COLS; j += 4)
@@ -432,7 +466,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
     } else {
         // ------------------------------------------------------------ epilogue
-        epilogue_role<Cf, BN>(p, tmem_base, tfull_bar, tempty_bar, abort_s, warp, lane);
+        epilogue_role<Cf, BN>(SingleSrc{p}, p.err, p.timeout, tmem_base, tfull_bar, tempty_bar, abort_s, warp, lane);
     }
 
     tc_fence_before();
@@ -822,9 +856,46 @@ struct CfgFused {
     static_assert(NCONV * 32 == BM && NCONV == NBOX, "one converter lane per A row and per B box row");
 };
 
-template <int MODE>
-__global__ void __launch_bounds__(CfgFused<MODE>::THREADS, 1)
-tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcParams p) {
+// Units of a grouped launch: device tables of problems, units (heaviest
+// first) and per-problem FP32 tensor maps.
+struct GroupSrc {
+    const TcGroupArgs& g;
+    __device__ __forceinline__ int64_t units() const { return g.nunits; }
+    // The r-th unit of this CTA: the units are sorted heaviest first and dealt
+    // in a snake order (forward in even rounds, backward in odd rounds), which
+    // evens out the sums of unequal units across CTAs.
+    __device__ __forceinline__ int64_t unit_of(int64_t r) const {
+        return r * gridDim.x + ((r & 1) ? (gridDim.x - 1 - blockIdx.x) : blockIdx.x);
+    }
+    __device__ __forceinline__ void get(int64_t u, UnitView& v) const {
+        const TcGroupUnit gu = g.units[u];
+        const TcGroupProblem& P = g.probs[gu.problem];
+        v.w.tm = gu.tm;
+        v.w.tn = gu.tn;
+        v.w.z = gu.z;
+        v.w.nsplit = P.splits;
+        v.w.kbeg = (int64_t)gu.z * P.kchunk;
+        v.w.kend = min(P.K, v.w.kbeg + P.kchunk);
+        v.w.sti = P.splits > 1 ? (int64_t)gu.tm * P.tiles_n + gu.tn : -1;
+        v.problem = gu.problem;
+        v.M = P.M; v.N = P.N; v.C = P.C; v.partial = P.partial; v.counters = P.counters;
+        v.max_splits = P.splits; v.chunk_kb = P.chunk_kb; v.reduce_after = 0;
+    }
+    __device__ __forceinline__ const void* map_a(const UnitView& v, const void*) const {
+        return static_cast<const char*>(g.maps) + 256 * (size_t)v.problem;
+    }
+    __device__ __forceinline__ const void* map_b(const UnitView& v, const void*) const {
+        return static_cast<const char*>(g.maps) + 256 * (size_t)v.problem + 128;
+    }
+    __device__ __forceinline__ void acquire(const void* a, const void* b) const {
+        tmap_acquire(a);
+        tmap_acquire(b);
+    }
+};
+
+template <int MODE, class Src>
+__device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, const void* tmB1, int* err,
+                                            long long timeout) {
     using Cf = CfgFused<MODE>;
     constexpr int BN = Cf::BN;
     extern __shared__ uint8_t smem_raw[];
@@ -854,7 +925,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         fence_mbar_init();
         fence_proxy_async();
     }
-    if (warp == 0 && lane == 0) { prefetch_tmap(&tmA); prefetch_tmap(&tmB); }
+    if (warp == 0 && lane == 0 && tmA1) { prefetch_tmap(tmA1); prefetch_tmap(tmB1); }
     if (warp == 1) { tmem_alloc(&tmem_base_s, Cf::TMEM_COLS); tmem_relinquish(); }
     tc_fence_before();
     __syncthreads();
@@ -862,7 +933,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
     const uint32_t tmem_base = tmem_base_s;
 
     auto fail = [&]() {
-        atomicOr(p.err, kErrTimeout);
+        atomicOr(err, kErrTimeout);
         abort_s = 1;
     };
     auto kblocks = [&](const Unit& w) -> int64_t { return (w.kend - w.kbeg + Cf::BK - 1) / Cf::BK; };
@@ -873,20 +944,25 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             int stage = 0;
             uint32_t phase = 0;
             int64_t issued = 0;
-            for (int64_t u = blockIdx.x; u < p.units && !abort_s; u += gridDim.x) {
-                const Unit w = decode_unit(p, u);
+            for (int64_t round = 0, u = src.unit_of(0); u < src.units() && !abort_s; u = src.unit_of(++round)) {
+                UnitView v;
+                src.get(u, v);
+                const Unit& w = v.w;
+                const void* mapA = src.map_a(v, tmA1);
+                const void* mapB = src.map_b(v, tmB1);
+                src.acquire(mapA, mapB);
                 const int64_t nkb = kblocks(w);
                 bool ok = true;
                 for (int64_t kb = 0; kb < nkb; kb++) {
-                    if (!mbar_wait_bounded(&st_empty[stage], phase ^ 1u, p.timeout)) { fail(); ok = false; break; }
+                    if (!mbar_wait_bounded(&st_empty[stage], phase ^ 1u, timeout)) { fail(); ok = false; break; }
                     if (abort_s) { ok = false; break; }
                     uint8_t* sa = stg + (size_t)stage * Cf::ST_STAGE;
                     mbar_arrive_expect_tx(&st_full[stage], (uint32_t)Cf::ST_STAGE);
                     const int32_t k = (int32_t)(w.kbeg + kb * Cf::BK);
-                    tma_load_2d(sa, &tmA, &st_full[stage], k, w.tm * Cf::BM);
+                    tma_load_2d(sa, mapA, &st_full[stage], k, w.tm * Cf::BM);
 #pragma unroll
                     for (int b = 0; b < Cf::NBOX; b++)
-                        tma_load_2d(sa + Cf::ST_A + b * Cf::ST_BOX, &tmB, &st_full[stage], w.tn * BN + 32 * b, k);
+                        tma_load_2d(sa + Cf::ST_A + b * Cf::ST_BOX, mapB, &st_full[stage], w.tn * BN + 32 * b, k);
                     issued++;
                     if (++stage == Cf::ST_STAGES) { stage = 0; phase ^= 1u; }
                 }
@@ -895,8 +971,8 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             // No copy may still be landing in shared memory when the CTA exits.
             const int64_t first = issued > Cf::ST_STAGES ? issued - Cf::ST_STAGES : 0;
             for (int64_t j = first; j < issued; j++) {
-                if (!mbar_wait_bounded(&st_full[j % Cf::ST_STAGES], (uint32_t)((j / Cf::ST_STAGES) & 1), p.timeout)) {
-                    atomicOr(p.err, kErrTimeout);
+                if (!mbar_wait_bounded(&st_full[j % Cf::ST_STAGES], (uint32_t)((j / Cf::ST_STAGES) & 1), timeout)) {
+                    atomicOr(err, kErrTimeout);
                     abort_s = 1;
                 }
             }
@@ -909,15 +985,17 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             int acc = 0;
             uint32_t acc_phase = 0;
             bool ok = true;
-            for (int64_t u = blockIdx.x; u < p.units && ok && !abort_s; u += gridDim.x) {
-                const int64_t nkb = kblocks(decode_unit(p, u));
-                for (int64_t kb0 = 0; kb0 < nkb && ok; kb0 += p.chunk_kb) {
-                    if (!mbar_wait_bounded(&tempty_bar[acc], acc_phase ^ 1u, p.timeout)) { fail(); ok = false; break; }
+            for (int64_t round = 0, u = src.unit_of(0); u < src.units() && ok && !abort_s; u = src.unit_of(++round)) {
+                UnitView v;
+                src.get(u, v);
+                const int64_t nkb = kblocks(v.w);
+                for (int64_t kb0 = 0; kb0 < nkb && ok; kb0 += v.chunk_kb) {
+                    if (!mbar_wait_bounded(&tempty_bar[acc], acc_phase ^ 1u, timeout)) { fail(); ok = false; break; }
                     tc_fence_after();
                     const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
-                    const int64_t kb1 = min(nkb, kb0 + (int64_t)p.chunk_kb);
+                    const int64_t kb1 = min(nkb, kb0 + (int64_t)v.chunk_kb);
                     for (int64_t kb = kb0; kb < kb1; kb++) {
-                        if (!mbar_wait_bounded(&op_full[stage], phase, p.timeout)) { fail(); ok = false; break; }
+                        if (!mbar_wait_bounded(&op_full[stage], phase, timeout)) { fail(); ok = false; break; }
                         tc_fence_after();
                         const uint32_t a_base = smem_u32(ops + (size_t)stage * Cf::OP_STAGE);
                         const uint32_t b_base = a_base + Cf::P * Cf::A_PLANE;
@@ -946,11 +1024,11 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
             }
             // No MMA may still be running when TMEM is freed.
             tc_commit(&done_bar);
-            if (!mbar_wait_bounded(&done_bar, 0u, p.timeout)) { atomicOr(p.err, kErrTimeout); abort_s = 1; }
+            if (!mbar_wait_bounded(&done_bar, 0u, timeout)) { atomicOr(err, kErrTimeout); abort_s = 1; }
         }
     } else if (warp < CONV0) {
         // ------------------------------------------------------------ epilogue
-        epilogue_role<Cf, BN>(p, tmem_base, tfull_bar, tempty_bar, abort_s, warp, lane);
+        epilogue_role<Cf, BN>(src, err, timeout, tmem_base, tfull_bar, tempty_bar, abort_s, warp, lane);
     } else {
         // ------------------------------------------------------------ converters
         // Warp cw splits A rows 32cw .. 32cw+31 (one per lane) and the 32 k
@@ -961,13 +1039,15 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         int stage = 0, ostage = 0;
         uint32_t phase = 0, ophase = 0;
         bool stop = false;
-        for (int64_t u = blockIdx.x; u < p.units && !stop; u += gridDim.x) {
-            const int64_t nkb = kblocks(decode_unit(p, u));
+        for (int64_t round = 0, u = src.unit_of(0); u < src.units() && !stop; u = src.unit_of(++round)) {
+            UnitView v;
+            src.get(u, v);
+            const int64_t nkb = kblocks(v.w);
             for (int64_t kb = 0; kb < nkb; kb++) {
                 int bad = abort_s;
                 if (!bad && lane == 0) {
-                    if (!mbar_wait_bounded(&op_empty[ostage], ophase ^ 1u, p.timeout) ||
-                        !mbar_wait_bounded(&st_full[stage], phase, p.timeout)) {
+                    if (!mbar_wait_bounded(&op_empty[ostage], ophase ^ 1u, timeout) ||
+                        !mbar_wait_bounded(&st_full[stage], phase, timeout)) {
                         fail();
                         bad = 1;
                     }
@@ -1039,6 +1119,14 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
         tc_fence_after();
         tmem_dealloc(tmem_base, Cf::TMEM_COLS);
     }
+}
+
+template <int MODE, bool GROUPED>
+__global__ void __launch_bounds__(CfgFused<MODE>::THREADS, 1)
+tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcParams p,
+                const TcGroupArgs g) {
+    if constexpr (GROUPED) fused_roles<MODE>(GroupSrc{g}, nullptr, nullptr, g.err, g.timeout);
+    else fused_roles<MODE>(SingleSrc{p}, &tmA, &tmB, p.err, p.timeout);
 }
 
 // Split-K reduction for plans that cut every tile into K slices. The GEMM
@@ -1334,41 +1422,49 @@ cudaError_t launch_cfg_pair(const TcArgs& a, cudaStream_t s) {
 // The fused-split kernel reads the FP32 operands directly: A as K x M rows of
 // 4-byte elements, B as N x K; both need rows of a multiple of 16 bytes and a
 // 16-byte aligned start (checked by the caller).
+bool encode_fused_maps(const float* A, const float* B, int64_t M, int64_t K, int64_t N, CUtensorMap* tmA,
+                       CUtensorMap* tmB) {
+    EncodeTiledFn enc = get_encode_fn();
+    if (!enc) return false;
+    constexpr int BK = CfgFused<MAXMULSK_PREC_BF16X6>::BK;
+    constexpr int BM = CfgFused<MAXMULSK_PREC_BF16X6>::BM;
+    const cuuint32_t estr[2] = {1, 1};
+    {
+        const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)M};
+        const cuuint64_t strides[1] = {(cuuint64_t)K * 4u};
+        const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
+        if (enc(tmA, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(A), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    {
+        const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)K};
+        const cuuint64_t strides[1] = {(cuuint64_t)N * 4u};
+        const cuuint32_t box[2] = {32u, (cuuint32_t)BK};
+        if (enc(tmB, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(B), dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    return true;
+}
+
 template <int MODE>
 cudaError_t launch_fused(const TcArgs& a, cudaStream_t s) {
     using Cf = CfgFused<MODE>;
     constexpr int BN = Cf::BN;
-    EncodeTiledFn enc = get_encode_fn();
-    if (!enc) return cudaErrorNotSupported;
     CUtensorMap tmA, tmB;
-    {
-        const cuuint64_t dims[2] = {(cuuint64_t)a.K, (cuuint64_t)a.M};
-        const cuuint64_t strides[1] = {(cuuint64_t)a.K * 4u};
-        const cuuint32_t box[2] = {(cuuint32_t)Cf::BK, (cuuint32_t)Cf::BM};
-        const cuuint32_t estr[2] = {1, 1};
-        if (enc(&tmA, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(a.A), dims, strides, box, estr,
-                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-            return cudaErrorInvalidValue;
-    }
-    {
-        const cuuint64_t dims[2] = {(cuuint64_t)a.N, (cuuint64_t)a.K};
-        const cuuint64_t strides[1] = {(cuuint64_t)a.N * 4u};
-        const cuuint32_t box[2] = {32u, (cuuint32_t)Cf::BK};
-        const cuuint32_t estr[2] = {1, 1};
-        if (enc(&tmB, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(a.B), dims, strides, box, estr,
-                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-            return cudaErrorInvalidValue;
-    }
+    if (!encode_fused_maps(a.A, a.B, a.M, a.K, a.N, &tmA, &tmB)) return cudaErrorInvalidValue;
     const Sched sc = make_sched(a.M, a.K, a.N, 128, BN, a.split_k, tc_slots(a.precision, 128, BN));
     const TcParams prm = make_params(a, sc, Cf::BK);
     if (sc.split_tiles > 0 && (!a.partial || !a.counters)) return cudaErrorInvalidValue;
 
     static std::atomic<uint64_t> smem_set{0};
-    cudaError_t e = set_smem_once(tc_fused_kernel<MODE>, Cf::SMEM, smem_set);
+    cudaError_t e = set_smem_once(tc_fused_kernel<MODE, false>, Cf::SMEM, smem_set);
     if (e != cudaSuccess) return e;
-    tc_fused_kernel<MODE><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, prm);
+    TcGroupArgs none{};
+    tc_fused_kernel<MODE, false><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, prm, none);
     e = cudaGetLastError();
     if (e != cudaSuccess || !prm.reduce_after) return e;
     return launch_reduce<BN>(prm, s);
@@ -1487,6 +1583,36 @@ cudaError_t tc_launch(const TcArgs& a, cudaStream_t s) {
         case MAXMULSK_PREC_BF16X9: return launch_mode<MAXMULSK_PREC_BF16X9>(a, s);
         default: return cudaErrorInvalidValue;
     }
+}
+
+bool tc_fused_maps(const float* A, const float* B, int64_t M, int64_t K, int64_t N, void* out) {
+    CUtensorMap* m = static_cast<CUtensorMap*>(out);
+    return encode_fused_maps(A, B, M, K, N, &m[0], &m[1]);
+}
+
+int tc_chunk_len(int64_t K, int splits) { return chunk_len(K, splits); }
+
+cudaError_t tc_grouped_launch(const TcGroupArgs& g, int precision, int grid, cudaStream_t s) {
+    static_assert(sizeof(CUtensorMap) == 128, "grouped tensor-map table stride");
+    if (g.nunits <= 0) return cudaSuccess;
+    CUtensorMap none{};
+    const TcParams p{};
+    if (precision == MAXMULSK_PREC_BF16X6) {
+        using Cf = CfgFused<MAXMULSK_PREC_BF16X6>;
+        static std::atomic<uint64_t> smem_set{0};
+        cudaError_t e = set_smem_once(tc_fused_kernel<MAXMULSK_PREC_BF16X6, true>, Cf::SMEM, smem_set);
+        if (e != cudaSuccess) return e;
+        tc_fused_kernel<MAXMULSK_PREC_BF16X6, true><<<(unsigned)grid, Cf::THREADS, Cf::SMEM, s>>>(none, none, p, g);
+    } else if (precision == MAXMULSK_PREC_BF16X9) {
+        using Cf = CfgFused<MAXMULSK_PREC_BF16X9>;
+        static std::atomic<uint64_t> smem_set{0};
+        cudaError_t e = set_smem_once(tc_fused_kernel<MAXMULSK_PREC_BF16X9, true>, Cf::SMEM, smem_set);
+        if (e != cudaSuccess) return e;
+        tc_fused_kernel<MAXMULSK_PREC_BF16X9, true><<<(unsigned)grid, Cf::THREADS, Cf::SMEM, s>>>(none, none, p, g);
+    } else {
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
 }
 
 }  // namespace mmsk

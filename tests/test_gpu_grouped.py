@@ -8,6 +8,7 @@ import pytest
 
 import maxmulsk_b200 as mm
 from maxmulsk_b200 import workloads
+from gpu_util import run_plan
 
 pytestmark = pytest.mark.gpu
 
@@ -105,6 +106,79 @@ def test_grouped_benchmark_batch_sampled(cuda, oracle_mod):
     assert mm.stream_status() == 0
     rng = np.random.default_rng(0)
     for i in rng.choice(len(shapes), 12, replace=False):
+        M, K, N = shapes[i]
+        ref = As[i].view(M, K).double() @ Bs[i].view(K, N).double()
+        err = float(torch.linalg.norm(Cs[i].view(M, N).double() - ref) /
+                    (torch.linalg.norm(As[i].double()) * torch.linalg.norm(Bs[i].double())))
+        assert err < 4 * 2.0 ** -24 * np.sqrt(K), (shapes[i], err)
+    for c in Cs:
+        assert not bool((c == SENT).any())
+    g.close()
+
+
+# K or N not a multiple of 4 (5, 999) runs in the FP32 part of the group.
+MIXED_TC = [(128, 1024, 128), (67, 68, 132), (300, 2048, 92), (1, 8192, 1024), (511, 640, 512), (20, 36, 40),
+            (3, 1000, 1000), (129, 4000, 256), (37, 5, 129), (64, 999, 100), (0, 16, 16), (16, 0, 16)]
+
+
+@pytest.mark.parametrize("prec", [mm.Precision.BF16X6, mm.Precision.BF16X9])
+def test_grouped_split_precision_matches_single_launches(cuda, oracle_mod, prec):
+    # One persistent fused-split tcgen05 kernel over the group: each problem's
+    # units are the tiles and K slices a single fused launch with the same K
+    # split computes, with the same chunked accumulation and slice order, so
+    # C is bit-identical to that launch. Problems the fused split cannot read
+    # run in the FP32 grouped kernel of the same graph: bit-exact against the
+    # oracle's panel order.
+    g, cbuf, host, offs = _group(cuda, oracle_mod, MIXED_TC, 700, mm.make_plan(prec, 128, 128, 0))
+    plan, splits, units = g.info()
+    assert plan.precision == int(prec) and plan.variant == mm.TC_FUSED_SPLIT and units > 0
+    assert g.launch() == 0
+    assert mm.stream_status() == 0
+    c = cbuf.cpu().numpy()
+    mask = np.ones(c.size, bool)
+    for (M, K, N), (A, B), off, s in zip(MIXED_TC, host, offs, splits):
+        got = c[off: off + M * N].reshape(M, N)
+        mask[off: off + M * N] = False
+        if M * N == 0:
+            continue
+        if K == 0:
+            assert np.all(got == 0)
+            continue
+        if K % 4 == 0 and N % 4 == 0:
+            st, want, _ = run_plan(cuda, A, B, M, K, N, mm.make_plan(prec, 128, 128, s, mm.TC_FUSED_SPLIT))
+            assert st == 0
+        else:
+            want = oracle_mod.sgemm_panels(A, B, M, K, N, kc=mm.slice_len(K, s), fma=True)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), ((M, K, N), s)
+    assert np.all(c[mask] == SENT), "a grouped launch wrote outside its C matrices"
+    # replays reproduce the result
+    first = cbuf.clone()
+    for off, (M, K, N) in zip(offs, MIXED_TC):
+        cbuf[off: off + M * N] = -7.0
+    for _ in range(2):
+        assert g.launch() == 0
+    cuda.cuda.synchronize()
+    assert bool(cuda.equal(first, cbuf))
+    g.close()
+
+
+def test_grouped_benchmark_batch_split_precision(cuda):
+    # The benchmark's 256-GEMM batch with BF16x6: FP32-class FP64 error on a
+    # sample, every C written.
+    torch = cuda
+    shapes = workloads.grouped_problems()
+    probs, As, Bs, Cs = [], [], [], []
+    for i, (M, K, N) in enumerate(shapes):
+        a = torch.rand(M * K, device="cuda") * 2 - 1
+        b = torch.rand(K * N, device="cuda") * 2 - 1
+        c = torch.full((M * N,), SENT, device="cuda")
+        probs.append((a, b, c, M, K, N))
+        As.append(a); Bs.append(b); Cs.append(c)
+    g = mm.Grouped(probs, mm.make_plan(mm.Precision.BF16X6, 128, 128, 0))
+    assert g.launch() == 0
+    assert mm.stream_status() == 0
+    rng = np.random.default_rng(1)
+    for i in rng.choice(len(shapes), 16, replace=False):
         M, K, N = shapes[i]
         ref = As[i].view(M, K).double() @ Bs[i].view(K, N).double()
         err = float(torch.linalg.norm(Cs[i].view(M, N).double() - ref) /
