@@ -26,6 +26,7 @@
 
 #include "internal.hpp"
 #include "runtime.hpp"
+#include "split_math.cuh"
 
 namespace mmsk {
 namespace {
@@ -306,38 +307,19 @@ sgemm_simt_grouped_kernel(const GroupProblem* __restrict__ probs, const GroupUni
 }
 
 // Split-K reduction for plans of three or more K slices: the slices wrote
-// their partial products ([slice][M][N]); each thread sums one output (four
-// adjacent columns where rows allow 128-bit access) over the slices in slice
-// order -- the order of the in-kernel fixup and of the reference's panel sum
-// C = p0 + p1 + ... -- so C is the same bit for bit. All outputs proceed in
-// parallel, instead of one CTA per tile walking its slices in turn.
-// HBM-bound: splits * M * N floats in, M * N out.
+// their partial products ([slice][M][N]); each thread sums one output over the
+// slices in slice order -- the order of the in-kernel fixup and of the
+// reference's panel sum C = p0 + p1 + ... -- so C is the same bit for bit. All
+// outputs proceed in parallel, 16 slice loads in flight per thread, instead of
+// one CTA per tile walking its slices in turn. HBM-bound: splits * M * N floats
+// in, M * N out.
 __global__ void __launch_bounds__(256)
 simt_splitk_reduce_kernel(const float* __restrict__ partial, float* __restrict__ C, int64_t M, int64_t N,
-                          int splits, int vec) {
+                          int splits) {
     const size_t MN = (size_t)M * (size_t)N;
-    const int64_t items = vec ? (int64_t)(MN / 4) : (int64_t)MN;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < items;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        if (vec) {
-            const float4* src = reinterpret_cast<const float4*>(partial) + i;
-            float4 acc = __ldcs(src);
-#pragma unroll 8
-            for (int z = 1; z < splits; z++) {
-                const float4 v = __ldcs(src + (size_t)z * (MN / 4));
-                acc.x = __fadd_rn(acc.x, v.x);
-                acc.y = __fadd_rn(acc.y, v.y);
-                acc.z = __fadd_rn(acc.z, v.z);
-                acc.w = __fadd_rn(acc.w, v.w);
-            }
-            reinterpret_cast<float4*>(C)[i] = acc;
-        } else {
-            float acc = __ldcs(partial + i);
-#pragma unroll 8
-            for (int z = 1; z < splits; z++) acc = __fadd_rn(acc, __ldcs(partial + (size_t)z * MN + i));
-            C[i] = acc;
-        }
-    }
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)MN;
+         i += (int64_t)gridDim.x * blockDim.x)
+        C[i] = ordered_sum(partial + i, MN, splits);
 }
 
 // Slices at or above which the partials are summed by the reduction kernel.
@@ -357,12 +339,10 @@ cudaError_t launch_tile(const SimtArgs& args, int variant, cudaStream_t s) {
     else sgemm_simt_kernel<BM, BN, false, false><<<grid, kThreads, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || !a.reduce_after) return e;
-    const int rvec = (a.N % 4 == 0) && ((uintptr_t)a.C % 16 == 0) && ((uintptr_t)a.partial % 16 == 0);
-    const int64_t items = rvec ? a.M * a.N / 4 : a.M * a.N;
-    int64_t blocks = (items + 255) / 256;
+    int64_t blocks = (a.M * a.N + 255) / 256;
     const int64_t cap = (int64_t)device_sm_count() * 8;
     if (cap > 0 && blocks > cap) blocks = cap;
-    simt_splitk_reduce_kernel<<<(unsigned)blocks, 256, 0, s>>>(a.partial, a.C, a.M, a.N, a.splits, rvec);
+    simt_splitk_reduce_kernel<<<(unsigned)blocks, 256, 0, s>>>(a.partial, a.C, a.M, a.N, a.splits);
     return cudaGetLastError();
 }
 

@@ -248,9 +248,13 @@ __device__ __forceinline__ void epilogue_role(const Src& src, int* err, long lon
 #pragma unroll
             for (int c = 0; c < COLS; c += Cf::LDW) {
                 uint32_t r[Cf::LDW];
+                if constexpr (Cf::LDW == 16) {
+                    tmem_ld_32x32b_x16(taddr + (uint32_t)c, r);
+                } else {
 #pragma unroll
-                for (int h = 0; h < Cf::LDW; h += 32)
-                    tmem_ld_32x32b_x32(taddr + (uint32_t)(c + h), *reinterpret_cast<uint32_t(*)[32]>(&r[h]));
+                    for (int h = 0; h < Cf::LDW; h += 32)
+                        tmem_ld_32x32b_x32(taddr + (uint32_t)(c + h), *reinterpret_cast<uint32_t(*)[32]>(&r[h]));
+                }
                 tmem_wait_ld();
                 if (kb0 == 0) {
 #pragma unroll
@@ -1131,47 +1135,29 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__
 
 // Split-K reduction for plans that cut every tile into K slices. The GEMM
 // wrote one partial tile per (128-row half, slice); each thread here sums one
-// float4 of a partial row over the slices in slice order -- the order of the
-// in-kernel fixup, so C is the same bit for bit -- and stores it. The slices
-// of a tile are read by many threads at once, instead of one warp walking
-// them in turn at the end of the GEMM. HBM-bound: nsplit partials in, C out.
+// element over the slices in slice order -- the order of the in-kernel fixup,
+// so C is the same bit for bit -- and stores it. The slices of a tile are
+// read by many threads at once, 16 loads in flight per thread, instead of one
+// warp walking them in turn at the end of the GEMM. HBM-bound: nsplit
+// partials in, C out.
 template <int BN>
 __global__ void __launch_bounds__(256)
 tc_splitk_reduce_kernel(const TcParams p) {
-    constexpr int Q = BN / 4;                                  // float4 per partial row
     constexpr size_t TILE = (size_t)128 * BN;
     const int halves = p.bm / 128;
-    const int64_t total = p.tiles * halves * 128 * Q;
-    const bool vec = (p.N % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0);
+    const int64_t total = p.tiles * halves * (int64_t)TILE;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int q4 = (int)(i % Q);
-        const int lrow = (int)((i / Q) % 128);
-        const int64_t th = i / ((int64_t)Q * 128);             // tile * halves + half
+        const int q = (int)(i % BN);
+        const int lrow = (int)((i / BN) % 128);
+        const int64_t th = i / (int64_t)TILE;                   // tile * halves + half
         int tm, tn;
         tile_coords(p, th / halves, tm, tn);
         const int64_t row = (int64_t)tm * p.bm + (th % halves) * 128 + lrow;
-        const int64_t col = (int64_t)tn * BN + q4 * 4;
+        const int64_t col = (int64_t)tn * BN + q;
         if (row >= p.M || col >= p.N) continue;
-        const float* src = p.partial + (size_t)th * p.max_splits * TILE + (size_t)lrow * BN + (size_t)q4 * 4;
-        float4 acc = __ldcs(reinterpret_cast<const float4*>(src));
-#pragma unroll 8
-        for (int z = 1; z < p.main_splits; z++) {
-            const float4 v = __ldcs(reinterpret_cast<const float4*>(src + (size_t)z * TILE));
-            acc.x = __fadd_rn(acc.x, v.x);
-            acc.y = __fadd_rn(acc.y, v.y);
-            acc.z = __fadd_rn(acc.z, v.z);
-            acc.w = __fadd_rn(acc.w, v.w);
-        }
-        float* dst = p.C + (size_t)row * (size_t)p.N + (size_t)col;
-        if (vec && col + 3 < p.N) {
-            *reinterpret_cast<float4*>(dst) = acc;
-        } else {
-            dst[0] = acc.x;
-            if (col + 1 < p.N) dst[1] = acc.y;
-            if (col + 2 < p.N) dst[2] = acc.z;
-            if (col + 3 < p.N) dst[3] = acc.w;
-        }
+        const float* src = p.partial + (size_t)th * p.max_splits * TILE + (size_t)lrow * BN + (size_t)q;
+        p.C[(size_t)row * (size_t)p.N + (size_t)col] = ordered_sum(src, TILE, p.main_splits);
     }
 }
 
@@ -1182,7 +1168,7 @@ constexpr int kReduceAfterSplits = 3;
 
 template <int BN>
 cudaError_t launch_reduce(const TcParams& prm, cudaStream_t s) {
-    const int64_t total = prm.tiles * (prm.bm / 128) * 128 * (BN / 4);
+    const int64_t total = prm.tiles * (prm.bm / 128) * 128 * BN;
     int64_t blocks = (total + 255) / 256;
     const int64_t cap = (int64_t)device_sm_count() * 8;
     if (cap > 0 && blocks > cap) blocks = cap;
