@@ -199,9 +199,11 @@ typedef struct maxmulsk_grouped_s* maxmulsk_grouped;
  * CUDA graph. Call with the device current.
  * A group_plan of precision MAXMULSK_PREC_BF16X6 / _BF16X9 / _SPLIT_AUTO
  * (= BF16X6) runs the problems on the fused-split tensor-core kernel, 128 x 128
- * tiles (tile and variant fields are ignored; split_k as for FP32); problems
- * with K or N not a multiple of 4, or A or B not 16-byte aligned, run in the
- * FP32 SIMT part of the same graph, at FP32 accuracy. */
+ * tiles (tile and variant fields are ignored; split_k as for FP32). An A with
+ * K not a multiple of 4 (or not 16-byte aligned) is copied to a padded buffer
+ * of the group inside the graph; problems with N not a multiple of 4, or B not
+ * 16-byte aligned, run in the FP32 SIMT part of the same graph, at FP32
+ * accuracy. */
 maxmulsk_status maxmulsk_grouped_create(const maxmulsk_problem* problems, size_t count,
                                         const maxmulsk_plan* group_plan, maxmulsk_grouped* out);
 /* Replays the captured graph on `stream` (asynchronous). */

@@ -11,11 +11,15 @@
 //     so that no unit is much longer than the average share of an SM;
 //   * split-precision groups (BF16x6 / BF16x9): the fused-split tcgen05 kernel
 //     (tc.cu, tc_fused_kernel) over tables of problems, units and per-problem
-//     FP32 tensor maps, 128 x 128 tiles. A problem the fused split cannot read
-//     (K or N not a multiple of 4, A or B not 16-byte aligned) runs in the FP32
-//     grouped kernel captured in the same graph, at FP32 accuracy.
+//     FP32 tensor maps, 128 x 128 tiles. TMA needs rows that start on 16-byte
+//     boundaries: an A whose K is not a multiple of 4 (or that is not 16-byte
+//     aligned) is copied, inside the same graph, into a zero-padded buffer of
+//     the group with rows of a multiple of 4 floats. A problem whose B cannot
+//     be read that way (N not a multiple of 4, B not 16-byte aligned) runs in
+//     the FP32 grouped kernel captured in the same graph, at FP32 accuracy.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -44,6 +48,13 @@ struct maxmulsk_grouped_s {
     size_t tc_counter_bytes = 0;
     void* tc_counters = nullptr;
     int tc_grid = 0;
+    struct Repack {                        // A copied to a 16-byte pitch before each launch
+        float* dst;
+        const float* src;
+        size_t rows, cols, dst_ld;
+    };
+    std::vector<Repack> repack;
+    void* d_apad = nullptr;
     // the captured graph
     cudaStream_t cap = nullptr;
     cudaGraph_t graph = nullptr;
@@ -204,7 +215,34 @@ maxmulsk_status build_tc(maxmulsk_grouped_s* g, const maxmulsk_problem* problems
             part_off[j] = partials;
             partials += align256(tc_group_partial_floats(tiles, splits) * sizeof(float));
         }
-        if (!tc_fused_maps(p.A, p.B, (int64_t)p.M, (int64_t)p.K, (int64_t)p.N, &maps[256 * j])) {
+    }
+    // A operands that TMA cannot read in place: one zero-padded buffer, rows
+    // of a multiple of 4 floats; the padding is never written and stays zero
+    // (the tensor maps' K bounds the loads in any case).
+    std::vector<size_t> pad_off(n, SIZE_MAX);
+    size_t pad_bytes = 0;
+    for (size_t j = 0; j < n; j++) {
+        const maxmulsk_problem& p = problems[idx[j]];
+        if (p.K % 4 == 0 && (uintptr_t)p.A % 16 == 0) continue;
+        pad_off[j] = pad_bytes;
+        pad_bytes += align256((size_t)p.M * ((p.K + 3) / 4 * 4) * sizeof(float));
+    }
+    if (pad_bytes) {
+        cudaError_t e = cudaMalloc(&g->d_apad, pad_bytes);
+        if (e == cudaSuccess) e = cudaMemset(g->d_apad, 0, pad_bytes);
+        if (e != cudaSuccess) return cuda_status(e, "grouped: padded A buffer");
+    }
+    for (size_t j = 0; j < n; j++) {
+        const maxmulsk_problem& p = problems[idx[j]];
+        const float* a = p.A;
+        int64_t lda = (int64_t)p.K;
+        if (pad_off[j] != SIZE_MAX) {
+            float* dst = reinterpret_cast<float*>(static_cast<char*>(g->d_apad) + pad_off[j]);
+            lda = (int64_t)((p.K + 3) / 4 * 4);
+            g->repack.push_back({dst, p.A, p.M, p.K, (size_t)lda});
+            a = dst;
+        }
+        if (!tc_fused_maps(a, lda, p.B, (int64_t)p.M, (int64_t)p.K, (int64_t)p.N, &maps[256 * j])) {
             set_error_message("grouped: tensor map encoding failed");
             return MAXMULSK_ERR_CUDA;
         }
@@ -268,8 +306,9 @@ maxmulsk_status build_tc(maxmulsk_grouped_s* g, const maxmulsk_problem* problems
     return MAXMULSK_OK;
 }
 
+// B is read in place by TMA; A, if it cannot be, is repacked (build_tc).
 bool fused_readable(const maxmulsk_problem& p) {
-    return p.K % 4 == 0 && p.N % 4 == 0 && ((uintptr_t)p.A % 16) == 0 && ((uintptr_t)p.B % 16) == 0;
+    return p.N % 4 == 0 && ((uintptr_t)p.B % 16) == 0;
 }
 
 }  // namespace
@@ -357,6 +396,11 @@ maxmulsk_status maxmulsk_grouped_create(const maxmulsk_problem* problems, size_t
             if (problems[i].M && problems[i].N && !problems[i].K)
                 cudaMemsetAsync(problems[i].C, 0, problems[i].M * problems[i].N * sizeof(float), g->cap);
         if (g->tc_counters && g->tc_counter_bytes) cudaMemsetAsync(g->tc_counters, 0, g->tc_counter_bytes, g->cap);
+        for (const auto& r : g->repack) {
+            cudaError_t ec = cudaMemcpy2DAsync(r.dst, r.dst_ld * sizeof(float), r.src, r.cols * sizeof(float),
+                                               r.cols * sizeof(float), r.rows, cudaMemcpyDeviceToDevice, g->cap);
+            if (ec != cudaSuccess) e = ec;
+        }
         if (g->tc.nunits > 0) {
             cudaError_t el = tc_grouped_launch(g->tc, tc_precision, g->tc_grid, g->cap);
             if (el != cudaSuccess) e = el;
@@ -402,6 +446,7 @@ void maxmulsk_grouped_destroy(maxmulsk_grouped g) {
     cudaFree(g->d_next);
     cudaFree(g->d_scratch);
     cudaFree(g->d_tc);
+    cudaFree(g->d_apad);
     delete g;
 }
 

@@ -115,9 +115,9 @@ struct TcGroupArgs {
     long long timeout;
 };
 // Encodes the two FP32 tensor maps the fused split reads for one problem
-// (A: K-contiguous rows, B: N-contiguous rows) into out[0..255]. K and N
-// multiples of 4, A and B 16-byte aligned.
-bool tc_fused_maps(const float* A, const float* B, int64_t M, int64_t K, int64_t N, void* out);
+// (A: K-contiguous rows lda floats apart, B: N-contiguous rows) into
+// out[0..255]. lda and N multiples of 4, A and B 16-byte aligned.
+bool tc_fused_maps(const float* A, int64_t lda, const float* B, int64_t M, int64_t K, int64_t N, void* out);
 // Chunk length (k's per TMEM accumulation) the kernels use for K and a K split.
 int tc_chunk_len(int64_t K, int splits);
 cudaError_t tc_grouped_launch(const TcGroupArgs& g, int precision, int grid, cudaStream_t s);

@@ -349,7 +349,6 @@ __global__ void __launch_bounds__(Cfg<MODE, BN>::THREADS, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                const TcParams p) {
     using Cf = Cfg<MODE, BN>;
-    constexpr int COLS = Cf::COLS;                   // columns of one epilogue thread
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[Cf::STAGES];
     __shared__ __align__(8) uint64_t empty_bar[Cf::STAGES];
@@ -832,7 +831,6 @@ cudaError_t set_smem_once(Kern kern, int bytes, std::atomic<uint64_t>& done) {
 // ============================================================================
 template <int MODE>
 struct CfgFused {
-    static constexpr bool TF32 = false;
     static constexpr int P = 3;                      // BF16 limb planes per operand
     static constexpr int ES = 2;
     static constexpr int BM = 128, BN = 128;
@@ -1408,8 +1406,8 @@ cudaError_t launch_cfg_pair(const TcArgs& a, cudaStream_t s) {
 // The fused-split kernel reads the FP32 operands directly: A as K x M rows of
 // 4-byte elements, B as N x K; both need rows of a multiple of 16 bytes and a
 // 16-byte aligned start (checked by the caller).
-bool encode_fused_maps(const float* A, const float* B, int64_t M, int64_t K, int64_t N, CUtensorMap* tmA,
-                       CUtensorMap* tmB) {
+bool encode_fused_maps(const float* A, int64_t lda, const float* B, int64_t M, int64_t K, int64_t N,
+                       CUtensorMap* tmA, CUtensorMap* tmB) {
     EncodeTiledFn enc = get_encode_fn();
     if (!enc) return false;
     constexpr int BK = CfgFused<MAXMULSK_PREC_BF16X6>::BK;
@@ -1417,7 +1415,7 @@ bool encode_fused_maps(const float* A, const float* B, int64_t M, int64_t K, int
     const cuuint32_t estr[2] = {1, 1};
     {
         const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)M};
-        const cuuint64_t strides[1] = {(cuuint64_t)K * 4u};
+        const cuuint64_t strides[1] = {(cuuint64_t)lda * 4u};
         const cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)BM};
         if (enc(tmA, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(A), dims, strides, box, estr,
                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -1441,7 +1439,7 @@ cudaError_t launch_fused(const TcArgs& a, cudaStream_t s) {
     using Cf = CfgFused<MODE>;
     constexpr int BN = Cf::BN;
     CUtensorMap tmA, tmB;
-    if (!encode_fused_maps(a.A, a.B, a.M, a.K, a.N, &tmA, &tmB)) return cudaErrorInvalidValue;
+    if (!encode_fused_maps(a.A, a.K, a.B, a.M, a.K, a.N, &tmA, &tmB)) return cudaErrorInvalidValue;
     const Sched sc = make_sched(a.M, a.K, a.N, 128, BN, a.split_k, tc_slots(a.precision, 128, BN));
     const TcParams prm = make_params(a, sc, Cf::BK);
     if (sc.split_tiles > 0 && (!a.partial || !a.counters)) return cudaErrorInvalidValue;
@@ -1571,9 +1569,9 @@ cudaError_t tc_launch(const TcArgs& a, cudaStream_t s) {
     }
 }
 
-bool tc_fused_maps(const float* A, const float* B, int64_t M, int64_t K, int64_t N, void* out) {
+bool tc_fused_maps(const float* A, int64_t lda, const float* B, int64_t M, int64_t K, int64_t N, void* out) {
     CUtensorMap* m = static_cast<CUtensorMap*>(out);
-    return encode_fused_maps(A, B, M, K, N, &m[0], &m[1]);
+    return encode_fused_maps(A, lda, B, M, K, N, &m[0], &m[1]);
 }
 
 int tc_chunk_len(int64_t K, int splits) { return chunk_len(K, splits); }

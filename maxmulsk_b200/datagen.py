@@ -3,7 +3,7 @@ generators: SplitMix64 of (seed, index), then
 
 * uniform : U[-1, 1) with 24-bit resolution, x = (u - 2^23) * 2^-23
 * normal  : Irwin-Hall sum of 12 24-bit uniforms (exact integer sum), centred,
-            rounded once to float32, times `scale` (BASELINE's N(0, 1/K) uses
+            rounded once to float32, times `scale` (the narrow-M inputs N(0, 1/K) use
             scale = 1/sqrt(K))
 * wide    : uniform 23-bit mantissa, exponent uniform in [-20, 20], random sign
 

@@ -163,7 +163,7 @@ def train_and_evaluate(d: dict, steps: int = 5000, lr: float = 1e-2, seeds=(0, 1
     """Model selection on the training shapes only: each seed is trained on
     the first n_train - n_val of them and scored (total-time + geometric-mean
     regret) on the last n_val; the best seed is retrained on all training
-    shapes and judged once on the held-out shapes, beside the rule."""
+    shapes and evaluated once on the held-out shapes, beside the rule."""
     n_train = int(d["n_train"])
     fit_rows, val_rows = np.arange(n_train - n_val), np.arange(n_train - n_val, n_train)
     test_rows = np.arange(n_train, len(d["shapes"]))

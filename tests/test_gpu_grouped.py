@@ -118,7 +118,9 @@ def test_grouped_benchmark_batch_sampled(cuda, oracle_mod):
     g.close()
 
 
-# K or N not a multiple of 4 (5, 999) runs in the FP32 part of the group.
+# N not a multiple of 4 (129) runs in the FP32 part of the group; K not a
+# multiple of 4 (5, 999) with a readable B runs on the tensor cores from a
+# repacked copy of A.
 MIXED_TC = [(128, 1024, 128), (67, 68, 132), (300, 2048, 92), (1, 8192, 1024), (511, 640, 512), (20, 36, 40),
             (3, 1000, 1000), (129, 4000, 256), (37, 5, 129), (64, 999, 100), (0, 16, 16), (16, 0, 16)]
 
@@ -128,9 +130,10 @@ def test_grouped_split_precision_matches_single_launches(cuda, oracle_mod, prec)
     # One persistent fused-split tcgen05 kernel over the group: each problem's
     # units are the tiles and K slices a single fused launch with the same K
     # split computes, with the same chunked accumulation and slice order, so
-    # C is bit-identical to that launch. Problems the fused split cannot read
-    # run in the FP32 grouped kernel of the same graph: bit-exact against the
-    # oracle's panel order.
+    # C is bit-identical to that launch (for K not a multiple of 4: to the
+    # split-inputs launch, whose planes are zero-padded in K the same way).
+    # Problems whose B the fused split cannot read run in the FP32 grouped
+    # kernel of the same graph: bit-exact against the oracle's panel order.
     g, cbuf, host, offs = _group(cuda, oracle_mod, MIXED_TC, 700, mm.make_plan(prec, 128, 128, 0))
     plan, splits, units = g.info()
     assert plan.precision == int(prec) and plan.variant == mm.TC_FUSED_SPLIT and units > 0
@@ -146,8 +149,9 @@ def test_grouped_split_precision_matches_single_launches(cuda, oracle_mod, prec)
         if K == 0:
             assert np.all(got == 0)
             continue
-        if K % 4 == 0 and N % 4 == 0:
-            st, want, _ = run_plan(cuda, A, B, M, K, N, mm.make_plan(prec, 128, 128, s, mm.TC_FUSED_SPLIT))
+        if N % 4 == 0:
+            variant = mm.TC_FUSED_SPLIT if K % 4 == 0 else mm.TC_SPLIT_INPUTS
+            st, want, _ = run_plan(cuda, A, B, M, K, N, mm.make_plan(prec, 128, 128, s, variant))
             assert st == 0
         else:
             want = oracle_mod.sgemm_panels(A, B, M, K, N, kc=mm.slice_len(K, s), fma=True)

@@ -96,7 +96,7 @@ def test_trained_picker_regret_on_held_out_shapes(cuda):
     # The learned picker end to end: the MLP trained by the library's CUDA
     # forward/backward/Adam kernels on the autotuner's measured timings of
     # 2000 random shapes (M, N, K log-uniform in [1, 16384]; both classes),
-    # then judged on the 500 held-out shapes against exhaustive search (the
+    # then evaluated on the 500 held-out shapes against exhaustive search (the
     # seed is chosen on a validation part of the training shapes). Bar:
     # within 5% of exhaustive time per shape (mean, geometric mean) and in
     # total, and better than the hand-written rule it replaces, timed in the
