@@ -26,12 +26,14 @@
 //               BK x BN in 128-byte column panels with 128-byte swizzle (BF16),
 //               into a ring of STAGES shared-memory stages.
 //   warp 1      TMEM owner; one thread issues the MMAs (128 x BN x KSTEP) of a
-//               chunk into one of two TMEM accumulators and commits each stage
-//               back to the producer and each chunk to the epilogue.
+//               chunk into one of NACC TMEM accumulators (all 512 columns: 4
+//               for tiles up to 128 columns wide, 2 for 256) and commits each
+//               stage back to the producer and each chunk to the epilogue.
 //   warps 2..   epilogue (4 or 8 warps): TMEM -> registers (tcgen05.ld
-//               32x32b), chunk sums in registers, then global stores. Two TMEM
-//               accumulators let the MMAs of one chunk overlap the drain of
-//               the previous one.
+//               32x32b), chunk sums in registers, then global stores. The MMAs
+//               run up to NACC - 1 chunks ahead of the drain, so the drain's
+//               latency stays off the tensor pipe even when a chunk is one
+//               stage long (K-split plans).
 // Work units are (output tile, K slice) pairs; with several slices per tile,
 // each slice writes a partial and the last slice to arrive (per warp's rows
 // and columns) sums the partials in slice order into C, deterministically.
@@ -82,7 +84,8 @@ struct Cfg {
     static constexpr int SMEM = STAGES * STAGE + 1024;
     static constexpr int NPROD = TF32 ? 3 : (MODE == MAXMULSK_PREC_BF16X6 ? 6 : 9);
     static constexpr uint32_t IDESC = make_idesc(TF32 ? 2u : 1u, 128u, (uint32_t)BN, B_KMAJOR ? 0u : 1u);
-    static constexpr uint32_t TMEM_COLS = 2 * BN;
+    static constexpr int NACC = (512 / BN) < 4 ? (512 / BN) : 4;   // TMEM accumulators
+    static constexpr uint32_t TMEM_COLS = NACC * BN;
     // Epilogue: 4 warps per TMEM lane quarter set; 8 for tiles of 128 columns
     // or more (two column groups), so each thread drains 64 or 128 columns.
     static constexpr int EPI = (BN >= 128) ? 8 : 4;
@@ -267,7 +270,7 @@ __device__ __forceinline__ void epilogue_role(const Src& src, int* err, long lon
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty_bar[acc]);
-            if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+            if (++acc == Cf::NACC) { acc = 0; acc_phase ^= 1u; }
         }
         if (stop) break;
 
@@ -352,8 +355,8 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[Cf::STAGES];
     __shared__ __align__(8) uint64_t empty_bar[Cf::STAGES];
-    __shared__ __align__(8) uint64_t tfull_bar[2];
-    __shared__ __align__(8) uint64_t tempty_bar[2];
+    __shared__ __align__(8) uint64_t tfull_bar[Cf::NACC];
+    __shared__ __align__(8) uint64_t tempty_bar[Cf::NACC];
     __shared__ __align__(8) uint64_t done_bar;
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
@@ -364,7 +367,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < Cf::STAGES; s++) { mbar_init(&full_bar[s], 1); mbar_init(&empty_bar[s], 1); }
-        for (int a = 0; a < 2; a++) { mbar_init(&tfull_bar[a], 1); mbar_init(&tempty_bar[a], Cf::EPI); }
+        for (int a = 0; a < Cf::NACC; a++) { mbar_init(&tfull_bar[a], 1); mbar_init(&tempty_bar[a], Cf::EPI); }
         mbar_init(&done_bar, 1);
         abort_s = 0;
         fence_mbar_init();
@@ -460,7 +463,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
                     }
                     if (!ok) break;
                     tc_commit(&tfull_bar[acc]);
-                    if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+                    if (++acc == Cf::NACC) { acc = 0; acc_phase ^= 1u; }
                 }
             }
             // No MMA may still be running when TMEM is freed.
@@ -849,7 +852,8 @@ struct CfgFused {
     static constexpr int SMEM = OP_STAGES * OP_STAGE + ST_STAGES * ST_STAGE + 1024;
     static constexpr int NPROD = (MODE == MAXMULSK_PREC_BF16X6) ? 6 : 9;
     static constexpr uint32_t IDESC = make_idesc(1u, 128u, (uint32_t)BN, 1u);
-    static constexpr uint32_t TMEM_COLS = 2 * BN;
+    static constexpr int NACC = 4;                   // TMEM accumulators (4 x 128 columns)
+    static constexpr uint32_t TMEM_COLS = NACC * BN;
     static constexpr int EPI = 8;                    // epilogue warps 2 .. 9
     static constexpr int COLS = BN * 4 / EPI;
     static constexpr int LDW = 32;
@@ -905,8 +909,8 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
     __shared__ __align__(8) uint64_t st_empty[Cf::ST_STAGES];
     __shared__ __align__(8) uint64_t op_full[Cf::OP_STAGES];
     __shared__ __align__(8) uint64_t op_empty[Cf::OP_STAGES];
-    __shared__ __align__(8) uint64_t tfull_bar[2];
-    __shared__ __align__(8) uint64_t tempty_bar[2];
+    __shared__ __align__(8) uint64_t tfull_bar[Cf::NACC];
+    __shared__ __align__(8) uint64_t tempty_bar[Cf::NACC];
     __shared__ __align__(8) uint64_t done_bar;
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
@@ -921,7 +925,7 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
     if (threadIdx.x == 0) {
         for (int s = 0; s < Cf::ST_STAGES; s++) { mbar_init(&st_full[s], 1); mbar_init(&st_empty[s], Cf::NCONV); }
         for (int s = 0; s < Cf::OP_STAGES; s++) { mbar_init(&op_full[s], Cf::NCONV); mbar_init(&op_empty[s], 1); }
-        for (int a = 0; a < 2; a++) { mbar_init(&tfull_bar[a], 1); mbar_init(&tempty_bar[a], Cf::EPI); }
+        for (int a = 0; a < Cf::NACC; a++) { mbar_init(&tfull_bar[a], 1); mbar_init(&tempty_bar[a], Cf::EPI); }
         mbar_init(&done_bar, 1);
         abort_s = 0;
         fence_mbar_init();
@@ -1021,7 +1025,7 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
                     }
                     if (!ok) break;
                     tc_commit(&tfull_bar[acc]);
-                    if (++acc == 2) { acc = 0; acc_phase ^= 1u; }
+                    if (++acc == Cf::NACC) { acc = 0; acc_phase ^= 1u; }
                 }
             }
             // No MMA may still be running when TMEM is freed.
