@@ -304,6 +304,15 @@ def run_tables(args) -> None:
             dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
             flops = 2.0 * M * N * K
             bytes_min = 4.0 * (M * K + K * N + M * N)
+            # The plain FP32 kernel: one FMA chain per output (split_k = 1; the
+            # tile does not change the bits), the error bar of the split modes.
+            # The picker's SIMT plan may cut K into slices, which is faster
+            # and also shortens the chains, so its error moves with the plan.
+            dCp = torch.empty(M * N, device="cuda")
+            fn_p, ws_p = run_plan(dA, dB, dCp, M, K, N, mm.make_plan(0, 128, 128, 1))
+            fn_p()
+            plain_err, _ = errors(dA, dB, dCp, M, K, N)
+            del ws_p, dCp
             simt_err = None
             for name, pc in kernels:
                 dC = torch.empty(M * N, device="cuda")
@@ -321,6 +330,7 @@ def run_tables(args) -> None:
                       "hbm_gbs_at_min_bytes": bytes_min / t / 1e9,
                       "frac_hbm_roofline": bytes_min / t / 1e9 / peaks["hbm_gbs"],
                       "normwise": nw, "max_rel": mr, "normwise_over_simt": nw / simt_err,
+                      "normwise_over_plain_fp32": nw / plain_err,
                       "peak_basis": ("FP32 FMA nominal at max clock" if pc == 0 else
                                      f"{peak_src} bf16 {peaks['bf16_tflops']} TF/s / {PRODUCTS[pc]}"
                                      + (" / 2 (TF32)" if pc == 1 else ""))})
@@ -614,7 +624,10 @@ def main() -> None:
             del mws
         out["speedup_vs_simt"] = (flops / t_step) / (flops / t_simt)
         out["speedup_vs_simt_gemm_only"] = t_simt / t_gemm
-        # ---- FP64-measured error of both kernels (cuBLAS DGEMM as the FP64 product, outside timing)
+        # ---- FP64-measured error of both kernels (cuBLAS DGEMM as the FP64 product, outside timing);
+        # the plain FP32 kernel (one FMA chain per output, split_k 1) is the error bar
+        dCp = torch.empty((M, N), dtype=torch.float32, device=dev)
+        mm.check(mm.sgemm_plan_dev(dA, dB, dCp, M, K, N, mm.make_plan(0, 128, 128, 1), None, 0, stream), "plain")
         if rank == 0:
             with torch.no_grad():
                 A64, B64 = dA.double(), dB.double()
@@ -622,14 +635,15 @@ def main() -> None:
                 floor = (A64.abs() @ B64.abs()) * 2.0 ** -24
                 nab = torch.linalg.norm(A64) * torch.linalg.norm(B64)
                 errs = {}
-                for name, Cx in [("tc", dC), ("simt", dCs)] + [(k, v["_C"]) for k, v in modes.items()]:
+                for name, Cx in [("tc", dC), ("simt", dCs), ("plain_fp32", dCp)] + [(k, v["_C"]) for k, v in modes.items()]:
                     d = (Cx.double() - C64).abs()
                     errs[name] = {"normwise": float(torch.linalg.norm(d) / nab),
                                   "max_rel": float((d / torch.maximum(C64.abs(), floor)).max())}
                 del A64, B64, C64, floor
             errs["tc_over_simt_normwise"] = errs["tc"]["normwise"] / errs["simt"]["normwise"]
-            out["fp64_error"] = {"tc": errs["tc"], "simt": errs["simt"],
-                                 "tc_over_simt_normwise": errs["tc_over_simt_normwise"]}
+            out["fp64_error"] = {"tc": errs["tc"], "simt": errs["simt"], "plain_fp32": errs["plain_fp32"],
+                                 "tc_over_simt_normwise": errs["tc_over_simt_normwise"],
+                                 "tc_over_plain_fp32_normwise": errs["tc"]["normwise"] / errs["plain_fp32"]["normwise"]}
             for k in modes:
                 modes[k]["normwise_over_simt"] = errs[k]["normwise"] / errs["simt"]["normwise"]
         for k in modes:

@@ -177,6 +177,14 @@ size_t maxmulsk_probe_split_bytes(size_t R, size_t C, int32_t precision, int32_t
 maxmulsk_status maxmulsk_probe_split_dev(const float* dX, size_t R, size_t C, int32_t precision,
                                          int32_t as_b, void* out, void* stream);
 
+/* TEST ONLY: launches one thread that waits, with the bounded wait every
+ * kernel of this library uses, on a barrier that nothing completes, for
+ * `cycles` SM clocks (1 .. 2e9); the timeout is then recorded in the device
+ * error word, which the next maxmulsk_stream_status(stream) reports as
+ * MAXMULSK_ERR_TIMEOUT and clears. No reference counterpart: the reference
+ * runs on the CPU and has no device-side waits. */
+maxmulsk_status maxmulsk_probe_timeout_dev(int64_t cycles, void* stream);
+
 /* ----------------------------------------------------------------------------
  * Grouped launches: many independent GEMMs in one persistent kernel, captured
  * in a CUDA graph. The counterpart of run_batch(const Gemm*, size_t)

@@ -93,6 +93,7 @@ _SIGNATURES: dict[str, tuple] = {
                                            c_void_p]),
     "maxmulsk_probe_split_bytes": (c_size_t, [c_size_t, c_size_t, c_int32, c_int32]),
     "maxmulsk_probe_split_dev": (c_int32, [c_void_p, c_size_t, c_size_t, c_int32, c_int32, c_void_p, c_void_p]),
+    "maxmulsk_probe_timeout_dev": (c_int32, [ctypes.c_int64, c_void_p]),
     "maxmulsk_stream_status": (c_int32, [c_void_p]),
     "maxmulsk_status_string": (c_char_p, [c_int32]),
     "maxmulsk_last_error_message": (c_char_p, []),

@@ -138,6 +138,14 @@ maxmulsk_status maxmulsk_probe_split_dev(const float* dX, size_t R, size_t C, in
                              "split pre-pass launch");
 }
 
+maxmulsk_status maxmulsk_probe_timeout_dev(int64_t cycles, void* stream) {
+    if (cycles <= 0 || cycles > 2000000000LL) { mmsk::set_error_message("cycles must be 1 .. 2e9"); return MAXMULSK_ERR_INVALID; }
+    int* err = mmsk::device_error_word();
+    if (!err) { mmsk::set_error_message("device error word unavailable"); return MAXMULSK_ERR_ALLOC; }
+    return mmsk::cuda_status(mmsk::tc_timeout_probe(err, (long long)cycles, static_cast<cudaStream_t>(stream)),
+                             "timeout probe launch");
+}
+
 maxmulsk_status maxmulsk_stream_status(void* stream) {
     return mmsk::stream_status(static_cast<cudaStream_t>(stream));
 }

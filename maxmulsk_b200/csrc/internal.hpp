@@ -144,6 +144,9 @@ size_t split_one_bytes(int64_t R, int64_t C, int precision, bool as_b);
 cudaError_t split_one(const float* X, int64_t R, int64_t C, int precision, bool as_b, void* out,
                       cudaStream_t s);
 
+// Test probe: a wait that nothing ends, bounded by `limit` SM clocks.
+cudaError_t tc_timeout_probe(int* err, long long limit, cudaStream_t s);
+
 // Number of SMs of the current device (cached).
 int device_sm_count();
 // Device error word of the current device (allocated on first use).

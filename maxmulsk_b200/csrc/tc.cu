@@ -1603,4 +1603,23 @@ cudaError_t tc_grouped_launch(const TcGroupArgs& g, int precision, int grid, cud
     return cudaGetLastError();
 }
 
+namespace {
+// One thread waits, with the kernels' bounded wait, on an mbarrier that no
+// one arrives at; when the limit runs out it records the timeout in the device
+// error word as the GEMM kernels do, and the kernel returns.
+__global__ void timeout_probe_kernel(int* err, long long limit) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+        if (!mbar_wait_bounded(&bar, 0u, limit)) atomicOr(err, kErrTimeout);
+    }
+}
+}  // namespace
+
+cudaError_t tc_timeout_probe(int* err, long long limit, cudaStream_t s) {
+    timeout_probe_kernel<<<1, 32, 0, s>>>(err, limit);
+    return cudaGetLastError();
+}
+
 }  // namespace mmsk
