@@ -94,7 +94,7 @@ struct Cfg {
     static constexpr int THREADS = 64 + 32 * EPI;
     static_assert(STAGES >= 2, "not enough shared memory for two stages");
     static_assert(COLS % 32 == 0, "column split must be whole");
-    static_assert(B_KMAJOR || BN % NBE == 0, "tile_n must be a whole number of 128-byte panels");
+    static_assert(B_KMAJOR || NBLK * NBE == BN, "tile_n must be a whole number of 128-byte panels");
 };
 
 // (A plane, B plane) of each product, in issue order.
@@ -520,7 +520,7 @@ struct CfgPair {
     static constexpr int LDW = (COLS >= 128) ? 32 : 64;
     static constexpr int THREADS = 64 + 32 * EPI;
     static_assert(STAGES >= 2, "not enough shared memory for two stages");
-    static_assert(B_KMAJOR || HN % NBE == 0, "half tile must be whole 128-byte panels");
+    static_assert(B_KMAJOR || HNBLK * NBE == HN, "half tile must be whole 128-byte panels");
     static_assert(COLS % 32 == 0, "column split must be whole");
 };
 
