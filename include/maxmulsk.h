@@ -39,8 +39,10 @@ typedef enum {
 /* ----------------------------------------------------------------------------
  * Drop-in entry points (host pointers, synchronous, FP32-SIMT accurate).
  * Each copies A and B to the current device, multiplies, copies C back and
- * waits. Pinned (page-locked) host buffers are copied directly; pageable ones
- * go through a pinned staging ring.
+ * waits. With page-locked A and C (cudaHostAlloc / cudaHostRegister) of at
+ * least 1024 rows and 32 MiB, the copies run as a pipeline of row blocks that
+ * overlaps them with the GEMM; pageable buffers are copied whole, through the
+ * CUDA runtime's own staging.
  * ------------------------------------------------------------------------- */
 
 /* Replaces capi/maxmulsk.h:32-33 (SMEKernels1x4AccKcOut). The plan comes from
