@@ -505,6 +505,24 @@ def main() -> None:
             mm.check(mm.sgemm_plan_dev(dA, dB, out, M, K, N, mp, mwp, mb, stream), "mode step")
         return step, mp, mws
 
+    # Plans: each kernel at its best plan for this shape, found by exhaustive
+    # search over the autotuner's candidates (maxmulsk_autotune_dev, untimed
+    # warm-up). The results go into the library's in-process tuning database,
+    # so maxmulsk_choose -- and the end-to-end call below -- return them.
+    tuned = {}
+    if fixed_plan is None:
+        tws_bytes = 2 << 30
+        tws = torch.empty(tws_bytes + 256, dtype=torch.uint8, device=dev)
+        twp = tws.data_ptr() + ((-tws.data_ptr()) % 256)
+        for pc in (0, 1, 2):
+            best, us = mm.Plan(), ctypes.c_float()
+            mm.check(mm.lib().maxmulsk_autotune_dev(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M, K, N, pc, twp,
+                                                    tws_bytes, ctypes.byref(best), ctypes.byref(us),
+                                                    stream.cuda_stream), "autotune")
+            tuned[pc] = (best.as_tuple(), float(us.value))
+        del tws
+        torch.cuda.synchronize(dev)
+
     # Split mode: the one given, or the fastest on this device (picked during
     # warm-up, untimed; every mode meets the accuracy bar at this shape).
     if args.precision == "auto":
@@ -573,7 +591,10 @@ def main() -> None:
                        f"{args.precision} split tensor-core kernel (split pre-pass + tcgen05 GEMM)") +
                        "; per-rank M-row shard",
                    "M": M, "K": K, "N": N, "precision": args.precision,
-                   "plan": {"tile_m": plan.tile_m, "tile_n": plan.tile_n, "split_k": plan.split_k},
+                   "plan": {"tile_m": plan.tile_m, "tile_n": plan.tile_n, "split_k": plan.split_k,
+                            "variant": plan.variant},
+                   "plan_search": "exhaustive over the autotuner's candidates at this shape (warm-up, untimed)"
+                                  if tuned else "given",
                    "l2": f"A+B+C = {4 * (M * K + K * N + M * N) / 2**20:.0f} MiB, workspace "
                          f"{ws_bytes / 2**20:.0f} MiB (L2 126 MB)", "parallelism": f"replicas x{world} (M-row shards)"},
         "clocks": clocks,
