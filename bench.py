@@ -417,7 +417,8 @@ def main() -> None:
     ap.add_argument("--precision", choices=["auto", "fp32"] + list(PREC), default="auto",
                     help="split mode; auto = the fastest mode on this device, picked during warm-up; "
                          "fp32 = the SIMT kernel as the timed step (profiling runs: no extras)")
-    ap.add_argument("--no-extras", action="store_true", help="headline timing only (for profiling runs)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline timing only, with the picker's plans (for profiling runs)")
     ap.add_argument("--shape", default=None, help="M,K,N instead of the square workload (profiling runs; "
                                                    "implies --no-extras)")
     ap.add_argument("--plan", default=None, help="precision,tile_m,tile_n,split_k instead of the picker's plan "
@@ -510,7 +511,7 @@ def main() -> None:
     # warm-up). The results go into the library's in-process tuning database,
     # so maxmulsk_choose -- and the end-to-end call below -- return them.
     tuned = {}
-    if fixed_plan is None:
+    if fixed_plan is None and not args.no_extras:     # profiling runs keep the picker's plans
         tws_bytes = 2 << 30
         tws = torch.empty(tws_bytes + 256, dtype=torch.uint8, device=dev)
         twp = tws.data_ptr() + ((-tws.data_ptr()) % 256)
