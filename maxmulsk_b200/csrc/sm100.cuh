@@ -1,5 +1,5 @@
 // Thin inline-PTX wrappers for the sm_100a features the tensor-core kernel
-// uses: mbarriers (with bounded waits), TMA tensor loads, tcgen05 (TMEM
+// uses: mbarriers (with bounded waits), TMA tensor loads and stores, tcgen05 (TMEM
 // allocation, MMA, commit, loads, fences) and the CTA-pair (cta_group::2)
 // forms of those. No load here takes the cluster multicast form; only the
 // tcgen05.commit arrival is multicast to the two CTAs of a pair.
@@ -76,6 +76,28 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, uint64_
         :: "r"(smem_u32(dst)), "l"(tmap), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
         : "memory");
 }
+// ---------------------------------------------------------------- TMA stores
+// Shared -> global through a tensor map; the box is clipped at the tensor's
+// extent, so a partial tile never writes outside the matrix. Completion is
+// tracked per issuing thread by bulk async-groups.
+__device__ __forceinline__ void tma_store_2d(const void* tmap, const void* src, int32_t c0, int32_t c1) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];"
+        :: "l"(tmap), "r"(smem_u32(src)), "r"(c0), "r"(c1)
+        : "memory");
+}
+__device__ __forceinline__ void bulk_commit_group() {
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// All of this thread's committed bulk stores have finished reading shared memory.
+__device__ __forceinline__ void bulk_wait_read_all() {
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+// All of this thread's committed bulk stores have completed.
+__device__ __forceinline__ void bulk_wait_all() {
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
 // A tensor map that lives in global memory (written by a copy, not passed as
 // a kernel parameter): make its current contents visible to the TMA unit.
 __device__ __forceinline__ void tmap_acquire(const void* tmap) {

@@ -49,6 +49,7 @@
 #include <cuda_runtime.h>
 #include <atomic>
 #include <cstdint>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -63,6 +64,13 @@ int tc_slots(int precision, int tile_m, int tile_n);
 namespace {
 
 using namespace sm100;
+
+// The TMA-store writeback stages one box of 32 rows x 32 FP32 columns
+// (128-byte rows) per epilogue warp. Dynamic shared memory a CTA may use:
+// 227 KB less 1 KB for the static barriers.
+constexpr int kStoreBox = 32;
+constexpr int kStoreWarpBytes = 32 * kStoreBox * 4;
+constexpr int kSmemCap = 227 * 1024 - 1024;
 
 template <int MODE, int BN>
 struct Cfg {
@@ -81,7 +89,7 @@ struct Cfg {
     static constexpr int STAGE = P * (A_PLANE + B_PLANE);
     static constexpr int STAGES_RAW = (220 * 1024) / STAGE;
     static constexpr int STAGES = STAGES_RAW > 8 ? 8 : STAGES_RAW;
-    static constexpr int SMEM = STAGES * STAGE + 1024;
+    static constexpr int RING = STAGES * STAGE;
     static constexpr int NPROD = TF32 ? 3 : (MODE == MAXMULSK_PREC_BF16X6 ? 6 : 9);
     static constexpr uint32_t IDESC = make_idesc(TF32 ? 2u : 1u, 128u, (uint32_t)BN, B_KMAJOR ? 0u : 1u);
     static constexpr int NACC = (512 / BN) < 4 ? (512 / BN) : 4;   // TMEM accumulators
@@ -92,6 +100,10 @@ struct Cfg {
     static constexpr int COLS = BN * 4 / EPI;        // columns per epilogue thread
     static constexpr int LDW = (COLS >= 128) ? 32 : 64;   // columns loaded per TMEM wait (register bound)
     static constexpr int THREADS = 64 + 32 * EPI;
+    // TMA-store writeback where its staging fits beside the ring without
+    // costing a stage (not BF16 tiles of 64 or 256 columns).
+    static constexpr bool TMA_STORE = RING + 1024 + EPI * kStoreWarpBytes <= kSmemCap;
+    static constexpr int SMEM = RING + 1024 + (TMA_STORE ? EPI * kStoreWarpBytes : 0);
     static_assert(STAGES >= 2, "not enough shared memory for two stages");
     static_assert(COLS % 32 == 0, "column split must be whole");
     static_assert(B_KMAJOR || NBLK * NBE == BN, "tile_n must be a whole number of 128-byte panels");
@@ -126,6 +138,7 @@ struct TcParams {
     int max_splits;
     int chunk_kb;            // stages per TMEM accumulation chunk
     int reduce_after;        // split tiles only write partials; tc_splitk_reduce_kernel sums them
+    int store_c;             // whole tiles leave through the C tensor map (TMA stores)
     float* C;
     float* partial;          // [split tile][slice][128 x BN], split tiles only
     unsigned* counters;      // EPI per split tile (one per epilogue warp)
@@ -195,7 +208,9 @@ struct UnitView {
 // Units of one GEMM (the schedule in TcParams).
 struct SingleSrc {
     const TcParams& p;
+    const CUtensorMap* tmC = nullptr;    // C for the TMA-store writeback, or none
     __device__ __forceinline__ int64_t units() const { return p.units; }
+    __device__ __forceinline__ const CUtensorMap* store_map(const UnitView&) const { return tmC; }
     // The r-th unit of this CTA: units are dealt round-robin.
     __device__ __forceinline__ int64_t unit_of(int64_t r) const { return r * gridDim.x + blockIdx.x; }
     __device__ __forceinline__ void get(int64_t u, UnitView& v) const {
@@ -209,15 +224,49 @@ struct SingleSrc {
     __device__ __forceinline__ void acquire(const void*, const void*) const {}
 };
 
+// One epilogue warp's 32 rows x COLS sums (thread `lane` holds row row0 +
+// lane, columns col0 ..) -> C by TMEM -> registers -> shared memory -> TMA
+// store, in boxes of 32 columns: the warp writes a box into `buf` with the
+// 128-byte swizzle (16-byte chunk c of row r at chunk c ^ (r & 7), so the
+// eight rows of each quarter-warp store hit eight different bank groups),
+// makes it visible to the async proxy, and lane 0 stores it. The box is
+// clipped at C's extent, so rows >= M and columns >= N are never written.
+// Before `buf` is rewritten lane 0 waits until its previous store has read
+// it; the caller waits for all of them before the CTA exits.
+template <int COLS>
+__device__ __forceinline__ void store_rows_tma(const CUtensorMap* tmC, uint8_t* buf, const float (&sum)[COLS],
+                                               int lane, int64_t row0, int64_t col0, int64_t M, int64_t N) {
+    if (row0 >= M) return;
+#pragma unroll
+    for (int b = 0; b < COLS; b += kStoreBox) {
+        if (col0 + b < N) {
+            if (lane == 0) bulk_wait_read_all();
+            __syncwarp();
+            uint8_t* rowp = buf + lane * (kStoreBox * 4);
+#pragma unroll
+            for (int c = 0; c < kStoreBox / 4; c++)
+                *reinterpret_cast<float4*>(rowp + ((c ^ (lane & 7)) << 4)) =
+                    make_float4(sum[b + 4 * c], sum[b + 4 * c + 1], sum[b + 4 * c + 2], sum[b + 4 * c + 3]);
+            fence_proxy_async();
+            __syncwarp();
+            if (lane == 0) {
+                tma_store_2d(tmC, buf, (int32_t)(col0 + b), (int32_t)row0);
+                bulk_commit_group();
+            }
+        }
+    }
+}
+
 // Epilogue warps of the one-CTA kernels: each TMEM chunk of a unit is drained
 // into FP32 register sums (round to nearest, chunk after chunk in k order);
-// then the unit's tile is stored, or, for a K slice, its partial tile, and the
-// last slice to arrive sums all slices in slice order (unless a separate
-// reduction kernel does that).
+// then the unit's tile is stored (by TMA stores through this warp's
+// buffer `cbuf` when the source gives a C tensor map, else from registers), or, for
+// a K slice, its partial tile, and the last slice to arrive sums all slices
+// in slice order (unless a separate reduction kernel does that).
 template <class Cf, int BN, class Src>
 __device__ __forceinline__ void epilogue_role(const Src& src, int* err, long long timeout, uint32_t tmem_base,
                                               uint64_t* tfull_bar, uint64_t* tempty_bar, volatile int& abort_s,
-                                              int warp, int lane) {
+                                              int warp, int lane, uint8_t* cbuf) {
     constexpr int COLS = Cf::COLS;                   // columns of one epilogue thread
     auto fail = [&]() {
         atomicOr(err, kErrTimeout);
@@ -280,7 +329,10 @@ __device__ __forceinline__ void epilogue_role(const Src& src, int* err, long lon
         const int64_t row = (int64_t)w.tm * Cf::BM + lrow;
         const int64_t col0 = (int64_t)w.tn * BN + lcol;
         if (w.sti < 0) {
-            if (row < M) {
+            const CUtensorMap* tmC = src.store_map(v);
+            if (cbuf && tmC) {
+                store_rows_tma<COLS>(tmC, cbuf, sum, lane, (int64_t)w.tm * Cf::BM + quarter * 32, col0, M, N);
+            } else if (row < M) {
                 float* dst = v.C + (size_t)row * (size_t)N + (size_t)col0;
                 if (vec && col0 + COLS <= N) {
 #pragma unroll
@@ -345,12 +397,14 @@ __device__ __forceinline__ void epilogue_role(const Src& src, int* err, long lon
             if (lane == 0) *ctr = 0u;
         }
     }
+    // This warp's TMA stores have completed before the CTA exits.
+    if (cbuf && lane == 0) bulk_wait_all();
 }
 
 template <int MODE, int BN>
 __global__ void __launch_bounds__(Cfg<MODE, BN>::THREADS, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-               const TcParams p) {
+               const __grid_constant__ CUtensorMap tmC, const TcParams p) {
     using Cf = Cfg<MODE, BN>;
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[Cf::STAGES];
@@ -373,7 +427,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         fence_mbar_init();
         fence_proxy_async();
     }
-    if (warp == 0 && lane == 0) { prefetch_tmap(&tmA); prefetch_tmap(&tmB); }
+    if (warp == 0 && lane == 0) {
+        prefetch_tmap(&tmA);
+        prefetch_tmap(&tmB);
+        if (p.store_c) prefetch_tmap(&tmC);
+    }
     if (warp == 1) { tmem_alloc(&tmem_base_s, Cf::TMEM_COLS); tmem_relinquish(); }
     tc_fence_before();
     __syncthreads();
@@ -472,7 +530,9 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
         }
     } else {
         // ------------------------------------------------------------ epilogue
-        epilogue_role<Cf, BN>(SingleSrc{p}, p.err, p.timeout, tmem_base, tfull_bar, tempty_bar, abort_s, warp, lane);
+        uint8_t* cbuf = (Cf::TMA_STORE && p.store_c) ? smem + Cf::RING + (warp - 2) * kStoreWarpBytes : nullptr;
+        epilogue_role<Cf, BN>(SingleSrc{p, p.store_c ? &tmC : nullptr}, p.err, p.timeout, tmem_base, tfull_bar,
+                              tempty_bar, abort_s, warp, lane, cbuf);
     }
 
     tc_fence_before();
@@ -511,7 +571,7 @@ struct CfgPair {
     static constexpr int STAGE = P * (A_PLANE + B_PLANE);
     static constexpr int STAGES_RAW = (220 * 1024) / STAGE;
     static constexpr int STAGES = STAGES_RAW > 8 ? 8 : STAGES_RAW;
-    static constexpr int SMEM = STAGES * STAGE + 1024;
+    static constexpr int RING = STAGES * STAGE;
     static constexpr int NPROD = TF32 ? 3 : (MODE == MAXMULSK_PREC_BF16X6 ? 6 : 9);
     static constexpr uint32_t IDESC = make_idesc(TF32 ? 2u : 1u, 256u, (uint32_t)BN, B_KMAJOR ? 0u : 1u);
     static constexpr uint32_t TMEM_COLS = 2 * BN;
@@ -519,6 +579,8 @@ struct CfgPair {
     static constexpr int COLS = BN * 4 / EPI;
     static constexpr int LDW = (COLS >= 128) ? 32 : 64;
     static constexpr int THREADS = 64 + 32 * EPI;
+    static constexpr bool TMA_STORE = RING + 1024 + EPI * kStoreWarpBytes <= kSmemCap;   // as Cfg
+    static constexpr int SMEM = RING + 1024 + (TMA_STORE ? EPI * kStoreWarpBytes : 0);
     static_assert(STAGES >= 2, "not enough shared memory for two stages");
     static_assert(B_KMAJOR || HNBLK * NBE == HN, "half tile must be whole 128-byte panels");
     static_assert(COLS % 32 == 0, "column split must be whole");
@@ -527,7 +589,7 @@ struct CfgPair {
 template <int MODE, int BN>
 __global__ void __launch_bounds__(CfgPair<MODE, BN>::THREADS, 1)
 tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                    const TcParams p) {
+                    const __grid_constant__ CUtensorMap tmC, const TcParams p) {
     using Cf = CfgPair<MODE, BN>;
     constexpr int COLS = Cf::COLS;
     extern __shared__ uint8_t smem_raw[];
@@ -555,7 +617,11 @@ tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
         fence_mbar_init();
         fence_proxy_async();
     }
-    if (warp == 0 && lane == 0) { prefetch_tmap(&tmA); prefetch_tmap(&tmB); }
+    if (warp == 0 && lane == 0) {
+        prefetch_tmap(&tmA);
+        prefetch_tmap(&tmB);
+        if (p.store_c) prefetch_tmap(&tmC);
+    }
     if (warp == 1) { tmem_alloc_pair(&tmem_base_s, Cf::TMEM_COLS); tmem_relinquish_pair(); }
     tc_fence_before();
     cluster_sync();                 // barriers of both CTAs initialised before any remote use
@@ -661,6 +727,7 @@ tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
         const int ew = warp - 2;
         const int quarter = warp & 3;
         const int cgroup = ew / 4;
+        uint8_t* cbuf = (Cf::TMA_STORE && p.store_c) ? smem + Cf::RING + ew * kStoreWarpBytes : nullptr;
         const int64_t M = p.M, N = p.N;
         const bool vec = (N % 4 == 0) && ((reinterpret_cast<uintptr_t>(p.C) & 15) == 0);
         const uint32_t tempty_leader0 = mapa_shared(&tempty_bar[0], 0);
@@ -708,7 +775,9 @@ tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
             const int64_t row = (int64_t)w.tm * Cf::BM + (int64_t)rank * Cf::HM + lrow;
             const int64_t col0 = (int64_t)w.tn * BN + lcol;
             if (w.sti < 0) {
-                if (row < M) {
+                if (cbuf) {
+                    store_rows_tma<COLS>(&tmC, cbuf, sum, lane, row - lane, col0, M, N);
+                } else if (row < M) {
                     float* dst = p.C + (size_t)row * (size_t)N + (size_t)col0;
                     if (vec && col0 + COLS <= N) {
 #pragma unroll
@@ -772,6 +841,7 @@ tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
                 if (lane == 0) *ctr = 0u;
             }
         }
+        if (cbuf && lane == 0) bulk_wait_all();       // this warp's TMA stores have completed
     }
 
     tc_fence_before();
@@ -849,7 +919,7 @@ struct CfgFused {
     static constexpr int NBOX = BN / 32;
     static constexpr int ST_STAGE = ST_A + NBOX * ST_BOX;
     static constexpr int ST_STAGES = 3;
-    static constexpr int SMEM = OP_STAGES * OP_STAGE + ST_STAGES * ST_STAGE + 1024;
+    static constexpr int RING = OP_STAGES * OP_STAGE + ST_STAGES * ST_STAGE;
     static constexpr int NPROD = (MODE == MAXMULSK_PREC_BF16X6) ? 6 : 9;
     static constexpr uint32_t IDESC = make_idesc(1u, 128u, (uint32_t)BN, 1u);
     static constexpr int NACC = 4;                   // TMEM accumulators (4 x 128 columns)
@@ -859,6 +929,8 @@ struct CfgFused {
     static constexpr int LDW = 32;
     static constexpr int NCONV = 4;                  // converter warps 10 .. 13
     static constexpr int THREADS = 64 + 32 * (EPI + NCONV);
+    static constexpr bool TMA_STORE = RING + 1024 + EPI * kStoreWarpBytes <= kSmemCap;   // as Cfg
+    static constexpr int SMEM = RING + 1024 + (TMA_STORE ? EPI * kStoreWarpBytes : 0);
     static_assert(NCONV * 32 == BM && NCONV == NBOX, "one converter lane per A row and per B box row");
 };
 
@@ -867,6 +939,8 @@ struct CfgFused {
 struct GroupSrc {
     const TcGroupArgs& g;
     __device__ __forceinline__ int64_t units() const { return g.nunits; }
+    // C of a grouped problem is written from registers.
+    __device__ __forceinline__ const CUtensorMap* store_map(const UnitView&) const { return nullptr; }
     // The r-th unit of this CTA: the units are sorted heaviest first and dealt
     // in a snake order (forward in even rounds, backward in odd rounds), which
     // evens out the sums of unequal units across CTAs.
@@ -900,8 +974,8 @@ struct GroupSrc {
 };
 
 template <int MODE, class Src>
-__device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, const void* tmB1, int* err,
-                                            long long timeout) {
+__device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, const void* tmB1, const void* tmC1,
+                                            int* err, long long timeout) {
     using Cf = CfgFused<MODE>;
     constexpr int BN = Cf::BN;
     extern __shared__ uint8_t smem_raw[];
@@ -931,7 +1005,11 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
         fence_mbar_init();
         fence_proxy_async();
     }
-    if (warp == 0 && lane == 0 && tmA1) { prefetch_tmap(tmA1); prefetch_tmap(tmB1); }
+    if (warp == 0 && lane == 0 && tmA1) {
+        prefetch_tmap(tmA1);
+        prefetch_tmap(tmB1);
+        if (tmC1) prefetch_tmap(tmC1);
+    }
     if (warp == 1) { tmem_alloc(&tmem_base_s, Cf::TMEM_COLS); tmem_relinquish(); }
     tc_fence_before();
     __syncthreads();
@@ -1034,7 +1112,8 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
         }
     } else if (warp < CONV0) {
         // ------------------------------------------------------------ epilogue
-        epilogue_role<Cf, BN>(src, err, timeout, tmem_base, tfull_bar, tempty_bar, abort_s, warp, lane);
+        uint8_t* cbuf = (Cf::TMA_STORE && tmC1) ? smem + Cf::RING + (warp - 2) * kStoreWarpBytes : nullptr;
+        epilogue_role<Cf, BN>(src, err, timeout, tmem_base, tfull_bar, tempty_bar, abort_s, warp, lane, cbuf);
     } else {
         // ------------------------------------------------------------ converters
         // Warp cw splits A rows 32cw .. 32cw+31 (one per lane) and the 32 k
@@ -1129,10 +1208,14 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
 
 template <int MODE, bool GROUPED>
 __global__ void __launch_bounds__(CfgFused<MODE>::THREADS, 1)
-tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, const TcParams p,
-                const TcGroupArgs g) {
-    if constexpr (GROUPED) fused_roles<MODE>(GroupSrc{g}, nullptr, nullptr, g.err, g.timeout);
-    else fused_roles<MODE>(SingleSrc{p}, &tmA, &tmB, p.err, p.timeout);
+tc_fused_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                const __grid_constant__ CUtensorMap tmC, const TcParams p, const TcGroupArgs g) {
+    if constexpr (GROUPED) {
+        fused_roles<MODE>(GroupSrc{g}, nullptr, nullptr, nullptr, g.err, g.timeout);
+    } else {
+        const CUtensorMap* c = p.store_c ? &tmC : nullptr;
+        fused_roles<MODE>(SingleSrc{p, c}, &tmA, &tmB, c, p.err, p.timeout);
+    }
 }
 
 // Split-K reduction for plans that cut every tile into K slices. The GEMM
@@ -1276,12 +1359,36 @@ TcParams make_params(const TcArgs& a, const Sched& sc, int bk) {
     prm.max_splits = sc.max_splits;
     prm.chunk_kb = chunk_len(a.K, sc.main_splits) / bk;
     prm.reduce_after = (sc.main_splits >= kReduceAfterSplits) ? 1 : 0;
+    prm.store_c = 0;
     prm.C = a.C;
     prm.partial = a.partial;
     prm.counters = a.counters;
     prm.err = a.err;
     prm.timeout = 2000000000LL;   // about one second at B200 clocks
     return prm;
+}
+
+// C as the TMA-store writeback sees it: M rows of N FP32, boxes of 32 x 32
+// with the 128-byte swizzle. Needs rows of a multiple of 16 bytes, a 16-byte
+// aligned C and 32-bit box coordinates; otherwise (false) whole tiles are
+// stored from registers.
+bool encode_c_map(float* C, int64_t M, int64_t N, CUtensorMap* tm) {
+    std::memset(tm, 0, sizeof *tm);
+    EncodeTiledFn enc = get_encode_fn();
+    if (!enc || M <= 0 || N <= 0 || M > INT32_MAX || N > INT32_MAX || N % 4 != 0 ||
+        (reinterpret_cast<uintptr_t>(C) & 15) != 0)
+        return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)M};
+    const cuuint64_t strides[1] = {(cuuint64_t)N * 4u};
+    const cuuint32_t box[2] = {(cuuint32_t)kStoreBox, 32u};
+    const cuuint32_t estr[2] = {1, 1};
+    if (enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+        std::memset(tm, 0, sizeof *tm);
+        return false;
+    }
+    return true;
 }
 
 template <int MODE, int BN>
@@ -1327,13 +1434,15 @@ cudaError_t launch_cfg(const TcArgs& a, cudaStream_t s) {
     }
 
     const Sched sc = make_sched(a.M, a.K, a.N, 128, BN, a.split_k, tc_slots(a.precision, 128, BN));
-    const TcParams prm = make_params(a, sc, Cf::BK);
+    TcParams prm = make_params(a, sc, Cf::BK);
     if (sc.split_tiles > 0 && (!a.partial || !a.counters)) return cudaErrorInvalidValue;
+    CUtensorMap tmC;
+    prm.store_c = (encode_c_map(a.C, a.M, a.N, &tmC) && Cf::TMA_STORE) ? 1 : 0;
 
     static std::atomic<uint64_t> smem_set{0};
     cudaError_t e = set_smem_once(tc_gemm_kernel<MODE, BN>, Cf::SMEM, smem_set);
     if (e != cudaSuccess) return e;
-    tc_gemm_kernel<MODE, BN><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, prm);
+    tc_gemm_kernel<MODE, BN><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, tmC, prm);
     e = cudaGetLastError();
     if (e != cudaSuccess || !prm.reduce_after) return e;
     return launch_reduce<BN>(prm, s);
@@ -1382,8 +1491,10 @@ cudaError_t launch_cfg_pair(const TcArgs& a, cudaStream_t s) {
     }
 
     const Sched sc = make_sched(a.M, a.K, a.N, 256, BN, a.split_k, tc_slots(a.precision, 256, BN));
-    const TcParams prm = make_params(a, sc, Cf::BK);
+    TcParams prm = make_params(a, sc, Cf::BK);
     if (sc.split_tiles > 0 && (!a.partial || !a.counters)) return cudaErrorInvalidValue;
+    CUtensorMap tmC;
+    prm.store_c = (encode_c_map(a.C, a.M, a.N, &tmC) && Cf::TMA_STORE) ? 1 : 0;
 
     static std::atomic<uint64_t> smem_set{0};
     cudaError_t e = set_smem_once(tc_gemm_pair_kernel<MODE, BN>, Cf::SMEM, smem_set);
@@ -1400,7 +1511,7 @@ cudaError_t launch_cfg_pair(const TcArgs& a, cudaStream_t s) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, tc_gemm_pair_kernel<MODE, BN>, tmA, tmB, prm);
+    e = cudaLaunchKernelEx(&cfg, tc_gemm_pair_kernel<MODE, BN>, tmA, tmB, tmC, prm);
     if (e != cudaSuccess) return e;
     e = cudaGetLastError();
     if (e != cudaSuccess || !prm.reduce_after) return e;
@@ -1445,14 +1556,16 @@ cudaError_t launch_fused(const TcArgs& a, cudaStream_t s) {
     CUtensorMap tmA, tmB;
     if (!encode_fused_maps(a.A, a.K, a.B, a.M, a.K, a.N, &tmA, &tmB)) return cudaErrorInvalidValue;
     const Sched sc = make_sched(a.M, a.K, a.N, 128, BN, a.split_k, tc_slots(a.precision, 128, BN));
-    const TcParams prm = make_params(a, sc, Cf::BK);
+    TcParams prm = make_params(a, sc, Cf::BK);
     if (sc.split_tiles > 0 && (!a.partial || !a.counters)) return cudaErrorInvalidValue;
+    CUtensorMap tmC;
+    prm.store_c = (encode_c_map(a.C, a.M, a.N, &tmC) && Cf::TMA_STORE) ? 1 : 0;
 
     static std::atomic<uint64_t> smem_set{0};
     cudaError_t e = set_smem_once(tc_fused_kernel<MODE, false>, Cf::SMEM, smem_set);
     if (e != cudaSuccess) return e;
     TcGroupArgs none{};
-    tc_fused_kernel<MODE, false><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, prm, none);
+    tc_fused_kernel<MODE, false><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, tmC, prm, none);
     e = cudaGetLastError();
     if (e != cudaSuccess || !prm.reduce_after) return e;
     return launch_reduce<BN>(prm, s);
@@ -1590,13 +1703,13 @@ cudaError_t tc_grouped_launch(const TcGroupArgs& g, int precision, int grid, cud
         static std::atomic<uint64_t> smem_set{0};
         cudaError_t e = set_smem_once(tc_fused_kernel<MAXMULSK_PREC_BF16X6, true>, Cf::SMEM, smem_set);
         if (e != cudaSuccess) return e;
-        tc_fused_kernel<MAXMULSK_PREC_BF16X6, true><<<(unsigned)grid, Cf::THREADS, Cf::SMEM, s>>>(none, none, p, g);
+        tc_fused_kernel<MAXMULSK_PREC_BF16X6, true><<<(unsigned)grid, Cf::THREADS, Cf::SMEM, s>>>(none, none, none, p, g);
     } else if (precision == MAXMULSK_PREC_BF16X9) {
         using Cf = CfgFused<MAXMULSK_PREC_BF16X9>;
         static std::atomic<uint64_t> smem_set{0};
         cudaError_t e = set_smem_once(tc_fused_kernel<MAXMULSK_PREC_BF16X9, true>, Cf::SMEM, smem_set);
         if (e != cudaSuccess) return e;
-        tc_fused_kernel<MAXMULSK_PREC_BF16X9, true><<<(unsigned)grid, Cf::THREADS, Cf::SMEM, s>>>(none, none, p, g);
+        tc_fused_kernel<MAXMULSK_PREC_BF16X9, true><<<(unsigned)grid, Cf::THREADS, Cf::SMEM, s>>>(none, none, none, p, g);
     } else {
         return cudaErrorInvalidValue;
     }

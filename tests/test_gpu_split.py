@@ -102,6 +102,31 @@ def test_tc_gemm_vs_exact_split_product(cuda, oracle_mod, prec, tile, split_k):
         assert np.max(np.abs(C - ideal)) <= K * 2.0 ** -22 + 1e-6
 
 
+WRITEBACK_SHAPES = [(300, 256, 200), (1, 64, 4), (129, 96, 260), (257, 128, 36), (128, 64, 128)]
+
+
+@pytest.mark.parametrize("prec", MODES)
+@pytest.mark.parametrize("tile", TC_TILES)
+def test_tma_store_writeback_equals_register_writeback(cuda, oracle_mod, prec, tile):
+    # Whole tiles leave through TMA stores when C is 16-byte aligned and N is
+    # a multiple of 4 (tile configurations with shared memory for the store
+    # boxes), and from registers otherwise -- here by placing C one float off
+    # its alignment. The sums are the same, so the bits are; the boxes
+    # clipped at the M and N edges write nothing outside C (guard bands).
+    variants = [0] + ([mm.TC_FUSED_SPLIT] if prec != mm.Precision.TF32X3 and tile == (128, 128) else [])
+    for i, (M, K, N) in enumerate(WRITEBACK_SHAPES):
+        A = oracle_mod.fill_uniform(M * K, 600 + i)
+        B = oracle_mod.fill_uniform(K * N, 700 + i)
+        dA, dB = to_dev(cuda, A), to_dev(cuda, B)
+        for var in variants:
+            plan = mm.make_plan(prec, tile[0], tile[1], 1, var)
+            st1, C1, b1 = run_plan(cuda, A, B, M, K, N, plan, dA=dA, dB=dB)
+            st2, C2, b2 = run_plan(cuda, A, B, M, K, N, plan, dA=dA, dB=dB, offset=1)
+            assert st1 == 0 and st2 == 0, mm.last_error_message()
+            assert b1 and b2, ((M, K, N), var)
+            assert np.array_equal(bits(C1), bits(C2)), ((M, K, N), var)
+
+
 @pytest.mark.parametrize("kind", ["uniform", "wide"])
 def test_split_error_within_twice_simt(cuda, oracle_mod, kind):
     # The bar is the plain FP32 kernel: one FMA chain per output (split_k 1).
