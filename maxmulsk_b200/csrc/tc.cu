@@ -929,7 +929,10 @@ struct CfgFused {
     static constexpr int LDW = 32;
     static constexpr int NCONV = 4;                  // converter warps 10 .. 13
     static constexpr int THREADS = 64 + 32 * (EPI + NCONV);
-    static constexpr bool TMA_STORE = RING + 1024 + EPI * kStoreWarpBytes <= kSmemCap;   // as Cfg
+    // Register writeback: at 448 threads the register cap is 128, and the
+    // store boxes' code made the epilogue spill (measured 2 % slower on
+    // 128 x 32768 x 512, whose C is 256 KB).
+    static constexpr bool TMA_STORE = false;
     static constexpr int SMEM = RING + 1024 + (TMA_STORE ? EPI * kStoreWarpBytes : 0);
     static_assert(NCONV * 32 == BM && NCONV == NBOX, "one converter lane per A row and per B box row");
 };
