@@ -257,6 +257,68 @@ __device__ __forceinline__ void store_rows_tma(const CUtensorMap* tmC, uint8_t* 
     }
 }
 
+// One thread's row segment of C (COLS columns from col0) from registers:
+// 128-bit stores where the segment and C allow them, else element by element
+// up to N. A row past M writes nothing.
+template <int COLS>
+__device__ __forceinline__ void store_row_regs(const float (&sum)[COLS], float* C, int64_t row, int64_t col0,
+                                               int64_t M, int64_t N, bool vec) {
+    if (row >= M) return;
+    float* dst = C + (size_t)row * (size_t)N + (size_t)col0;
+    if (vec && col0 + COLS <= N) {
+#pragma unroll
+        for (int j = 0; j < COLS; j += 4)
+            *reinterpret_cast<float4*>(dst + j) = make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
+    } else {
+#pragma unroll
+        for (int j = 0; j < COLS; j++)
+            if (col0 + j < N) dst[j] = sum[j];
+    }
+}
+
+// A K slice z of a split tile: this thread's row segment goes into the
+// slice's partial tile (`seg` = the segment in slice 0; slices `tile` floats
+// apart, compact whole rows). Unless a reduction kernel sums the slices
+// (`reduce_after`), the last slice to arrive on this warp's counter reads
+// every slice back in slice order (its own included, 128-bit loads), sums
+// them with round-to-nearest adds, stores the segment of C and resets the
+// counter.
+template <int COLS>
+__device__ __forceinline__ void finish_slice(float (&sum)[COLS], float* seg, size_t tile, int z, int nsplit,
+                                             bool reduce_after, unsigned* ctr, int lane, float* C, int64_t row,
+                                             int64_t col0, int64_t M, int64_t N, bool vec) {
+    float* part = seg + (size_t)z * tile;
+#pragma unroll
+    for (int j = 0; j < COLS; j += 4)
+        __stcg(reinterpret_cast<float4*>(part + j), make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]));
+    if (reduce_after) return;
+    __threadfence();
+    __syncwarp();
+    int last = 0;
+    if (lane == 0) last = (atomicAdd(ctr, 1u) == (unsigned)(nsplit - 1));
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return;
+    __threadfence();
+#pragma unroll
+    for (int j = 0; j < COLS; j += 4) {
+        const float4 t = __ldcg(reinterpret_cast<const float4*>(seg + j));
+        sum[j] = t.x; sum[j + 1] = t.y; sum[j + 2] = t.z; sum[j + 3] = t.w;
+    }
+    for (int q = 1; q < nsplit; q++) {
+        const float* bq = seg + (size_t)q * tile;
+#pragma unroll
+        for (int j = 0; j < COLS; j += 4) {
+            const float4 t = __ldcg(reinterpret_cast<const float4*>(bq + j));
+            sum[j] = __fadd_rn(sum[j], t.x);
+            sum[j + 1] = __fadd_rn(sum[j + 1], t.y);
+            sum[j + 2] = __fadd_rn(sum[j + 2], t.z);
+            sum[j + 3] = __fadd_rn(sum[j + 3], t.w);
+        }
+    }
+    store_row_regs<COLS>(sum, C, row, col0, M, N, vec);
+    if (lane == 0) *ctr = 0u;
+}
+
 // Epilogue warps of the one-CTA kernels: each TMEM chunk of a unit is drained
 // into FP32 register sums (round to nearest, chunk after chunk in k order);
 // then the unit's tile is stored (by TMA stores through this warp's
@@ -330,72 +392,14 @@ __device__ __forceinline__ void epilogue_role(const Src& src, int* err, long lon
         const int64_t col0 = (int64_t)w.tn * BN + lcol;
         if (w.sti < 0) {
             const CUtensorMap* tmC = src.store_map(v);
-            if (cbuf && tmC) {
-                store_rows_tma<COLS>(tmC, cbuf, sum, lane, (int64_t)w.tm * Cf::BM + quarter * 32, col0, M, N);
-            } else if (row < M) {
-                float* dst = v.C + (size_t)row * (size_t)N + (size_t)col0;
-                if (vec && col0 + COLS <= N) {
-#pragma unroll
-                    for (int j = 0; j < COLS; j += 4)
-                        *reinterpret_cast<float4*>(dst + j) = make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
-                } else {
-#pragma unroll
-                    for (int j = 0; j < COLS; j++)
-                        if (col0 + j < N) dst[j] = sum[j];
-                }
-            }
+            if (cbuf && tmC) store_rows_tma<COLS>(tmC, cbuf, sum, lane, row - lane, col0, M, N);
+            else store_row_regs<COLS>(sum, v.C, row, col0, M, N, vec);
             continue;
         }
-        // A slice of a split tile: write the partial tile (compact, whole
-        // rows), then the last slice to arrive for this warp's rows and
-        // columns sums all slices in slice order into C.
         constexpr size_t TILE = (size_t)Cf::BM * BN;
-        float* part = v.partial + ((size_t)w.sti * v.max_splits + w.z) * TILE + (size_t)lrow * BN + lcol;
-#pragma unroll
-        for (int j = 0; j < COLS; j += 4)
-            __stcg(reinterpret_cast<float4*>(part + j), make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]));
-        if (v.reduce_after) continue;        // summed by tc_splitk_reduce_kernel
-        __threadfence();
-        __syncwarp();
-        int last = 0;
-        unsigned* ctr = v.counters + (size_t)w.sti * Cf::EPI + ew;
-        if (lane == 0) last = (atomicAdd(ctr, 1u) == (unsigned)(w.nsplit - 1));
-        last = __shfl_sync(0xffffffffu, last, 0);
-        if (last) {
-            // Every slice of this thread's row segment, in slice order,
-            // read back with 128-bit loads (its own slice included).
-            __threadfence();
-            const float* base = v.partial + (size_t)w.sti * v.max_splits * TILE + (size_t)lrow * BN + lcol;
-#pragma unroll
-            for (int j = 0; j < COLS; j += 4) {
-                const float4 t = __ldcg(reinterpret_cast<const float4*>(base + j));
-                sum[j] = t.x; sum[j + 1] = t.y; sum[j + 2] = t.z; sum[j + 3] = t.w;
-            }
-            for (int q = 1; q < w.nsplit; q++) {
-                const float* bq = base + (size_t)q * TILE;
-#pragma unroll
-                for (int j = 0; j < COLS; j += 4) {
-                    const float4 t = __ldcg(reinterpret_cast<const float4*>(bq + j));
-                    sum[j] = __fadd_rn(sum[j], t.x);
-                    sum[j + 1] = __fadd_rn(sum[j + 1], t.y);
-                    sum[j + 2] = __fadd_rn(sum[j + 2], t.z);
-                    sum[j + 3] = __fadd_rn(sum[j + 3], t.w);
-                }
-            }
-            if (row < M) {
-                float* dst = v.C + (size_t)row * (size_t)N + (size_t)col0;
-                if (vec && col0 + COLS <= N) {
-#pragma unroll
-                    for (int j = 0; j < COLS; j += 4)
-                        *reinterpret_cast<float4*>(dst + j) = make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
-                } else {
-#pragma unroll
-                    for (int j = 0; j < COLS; j++)
-                        if (col0 + j < N) dst[j] = sum[j];
-                }
-            }
-            if (lane == 0) *ctr = 0u;
-        }
+        finish_slice<COLS>(sum, v.partial + (size_t)w.sti * v.max_splits * TILE + (size_t)lrow * BN + lcol, TILE, w.z,
+                           w.nsplit, v.reduce_after != 0, v.counters + (size_t)w.sti * Cf::EPI + ew, lane, v.C, row,
+                           col0, M, N, vec);
     }
     // This warp's TMA stores have completed before the CTA exits.
     if (cbuf && lane == 0) bulk_wait_all();
@@ -775,71 +779,16 @@ tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
             const int64_t row = (int64_t)w.tm * Cf::BM + (int64_t)rank * Cf::HM + lrow;
             const int64_t col0 = (int64_t)w.tn * BN + lcol;
             if (w.sti < 0) {
-                if (cbuf) {
-                    store_rows_tma<COLS>(&tmC, cbuf, sum, lane, row - lane, col0, M, N);
-                } else if (row < M) {
-                    float* dst = p.C + (size_t)row * (size_t)N + (size_t)col0;
-                    if (vec && col0 + COLS <= N) {
-#pragma unroll
-                        for (int j = 0; j < COLS; j += 4)
-                            *reinterpret_cast<float4*>(dst + j) = make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < COLS; j++)
-                            if (col0 + j < N) dst[j] = sum[j];
-                    }
-                }
+                if (cbuf) store_rows_tma<COLS>(&tmC, cbuf, sum, lane, row - lane, col0, M, N);
+                else store_row_regs<COLS>(sum, p.C, row, col0, M, N, vec);
                 continue;
             }
             // K-split tile: this CTA's 128-row half is its own partial tile.
             constexpr size_t TILE = (size_t)Cf::HM * BN;
             const int64_t half = w.sti * 2 + rank;
-            float* part = p.partial + ((size_t)half * p.max_splits + w.z) * TILE + (size_t)lrow * BN + lcol;
-#pragma unroll
-            for (int j = 0; j < COLS; j += 4)
-                __stcg(reinterpret_cast<float4*>(part + j), make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]));
-            if (p.reduce_after) continue;        // summed by tc_splitk_reduce_kernel
-            __threadfence();
-            __syncwarp();
-            int last = 0;
-            unsigned* ctr = p.counters + (size_t)half * Cf::EPI + ew;
-            if (lane == 0) last = (atomicAdd(ctr, 1u) == (unsigned)(w.nsplit - 1));
-            last = __shfl_sync(0xffffffffu, last, 0);
-            if (last) {
-                // Every slice of this thread's row segment, in slice order,
-                // read back with 128-bit loads (its own slice included).
-                __threadfence();
-                const float* base = p.partial + (size_t)half * p.max_splits * TILE + (size_t)lrow * BN + lcol;
-#pragma unroll
-                for (int j = 0; j < COLS; j += 4) {
-                    const float4 t = __ldcg(reinterpret_cast<const float4*>(base + j));
-                    sum[j] = t.x; sum[j + 1] = t.y; sum[j + 2] = t.z; sum[j + 3] = t.w;
-                }
-                for (int q = 1; q < w.nsplit; q++) {
-                    const float* bq = base + (size_t)q * TILE;
-#pragma unroll
-                    for (int j = 0; j < COLS; j += 4) {
-                        const float4 t = __ldcg(reinterpret_cast<const float4*>(bq + j));
-                        sum[j] = __fadd_rn(sum[j], t.x);
-                        sum[j + 1] = __fadd_rn(sum[j + 1], t.y);
-                        sum[j + 2] = __fadd_rn(sum[j + 2], t.z);
-                        sum[j + 3] = __fadd_rn(sum[j + 3], t.w);
-                    }
-                }
-                if (row < M) {
-                    float* dst = p.C + (size_t)row * (size_t)N + (size_t)col0;
-                    if (vec && col0 + COLS <= N) {
-#pragma unroll
-                        for (int j = 0; j < COLS; j += 4)
-                            *reinterpret_cast<float4*>(dst + j) = make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]);
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < COLS; j++)
-                            if (col0 + j < N) dst[j] = sum[j];
-                    }
-                }
-                if (lane == 0) *ctr = 0u;
-            }
+            finish_slice<COLS>(sum, p.partial + (size_t)half * p.max_splits * TILE + (size_t)lrow * BN + lcol, TILE,
+                               w.z, w.nsplit, p.reduce_after != 0, p.counters + (size_t)half * Cf::EPI + ew, lane, p.C,
+                               row, col0, M, N, vec);
         }
         if (cbuf && lane == 0) bulk_wait_all();       // this warp's TMA stores have completed
     }
