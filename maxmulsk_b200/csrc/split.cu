@@ -83,6 +83,59 @@ split_kernel(const float* __restrict__ src, int64_t R, int64_t Cin, int64_t Cout
     }
 }
 
+// B (K x N, row-major) -> BF16 limb planes in 128-byte column panels
+// [P][Np/64][K][64] (columns >= N zero). Block unit (panel g, chunk of 64
+// rows): 64 rows x 64 columns in, one contiguous 8 KB run of panel g per
+// plane out. Units are numbered panel-fastest, so the blocks running at one
+// time read whole rows of B, and every plane is written in long runs
+// instead of 128-byte pieces one panel (K x 128 bytes) apart, which is what
+// the row-major walk of split_kernel writes. A warp reads two 256-byte row
+// segments and writes 256 contiguous bytes per plane; each thread takes 4
+// quads, loads first.
+__global__ void __launch_bounds__(256)
+split_bf16_panels_kernel(const float* __restrict__ src, int64_t R, int64_t Cin, int64_t Cout,
+                         void* __restrict__ planes, size_t plane_bytes) {
+    constexpr int PANEL = 64, ROWS = 64, QUADS = PANEL / 4, PER = ROWS * QUADS / 256;
+    const int64_t npan = Cout / PANEL;
+    const int64_t units = npan * ((R + ROWS - 1) / ROWS);
+    const bool vec = (Cin % 4 == 0) && (((uintptr_t)src & 15) == 0);
+    for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+        const int64_t g = u % npan, r0 = (u / npan) * ROWS;
+        float x[PER][4];
+#pragma unroll
+        for (int i = 0; i < PER; i++) {
+            const int idx = threadIdx.x + i * 256;
+            const int64_t r = r0 + idx / QUADS, c = g * PANEL + (idx % QUADS) * 4;
+            const float* row = src + r * Cin;
+            if (r >= R) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) x[i][j] = 0.0f;
+            } else if (vec && c + 3 < Cin) {
+                const float4 v = __ldcs(reinterpret_cast<const float4*>(row + c));
+                x[i][0] = v.x; x[i][1] = v.y; x[i][2] = v.z; x[i][3] = v.w;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; j++) x[i][j] = (c + j < Cin) ? __ldcs(row + c + j) : 0.0f;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < PER; i++) {
+            const int idx = threadIdx.x + i * 256;
+            const int64_t r = r0 + idx / QUADS;
+            if (r >= R) continue;
+            const size_t off = ((size_t)g * (size_t)R + (size_t)r) * PANEL + (size_t)(idx % QUADS) * 4;
+            uint2 l[3];
+            bf16_limbs2(x[i][0], x[i][1], l[0].x, l[1].x, l[2].x);
+            bf16_limbs2(x[i][2], x[i][3], l[0].y, l[1].y, l[2].y);
+#pragma unroll
+            for (int p = 0; p < 3; p++) {
+                uint16_t* dst = reinterpret_cast<uint16_t*>(reinterpret_cast<char*>(planes) + (size_t)p * plane_bytes);
+                *reinterpret_cast<uint2*>(dst + off) = l[p];
+            }
+        }
+    }
+}
+
 // B (K x N, row-major) -> TF32 planes of B transposed, [P][N][Kp] with
 // k >= K zero. 32 x 32 tiles through shared memory so that both the read
 // (along n) and the write (along k) are coalesced.
@@ -128,6 +181,12 @@ cudaError_t launch_one(const float* src, int64_t R, int64_t Cin, int64_t Cout, i
     const int64_t total = R * (Cout / 4);
     if (total == 0) return cudaSuccess;
     const int sms = device_sm_count();
+    if (MODE != MAXMULSK_PREC_3XTF32 && panel == 64) {
+        const int64_t units = (Cout / 64) * ((R + 63) / 64);
+        const int64_t blocks = units < (int64_t)sms * 8 ? units : (int64_t)sms * 8;
+        split_bf16_panels_kernel<<<(unsigned)blocks, 256, 0, s>>>(src, R, Cin, Cout, planes, plane_bytes);
+        return cudaGetLastError();
+    }
     int64_t blocks = (total + 255) / 256;
     const int64_t cap = (int64_t)sms * 8;
     if (blocks > cap) blocks = cap;
