@@ -30,17 +30,20 @@
 //               for tiles up to 128 columns wide, 2 for 256) and commits each
 //               stage back to the producer and each chunk to the epilogue.
 //   warps 2..   epilogue (4 or 8 warps): TMEM -> registers (tcgen05.ld
-//               32x32b), chunk sums in registers, then global stores. The MMAs
-//               run up to NACC - 1 chunks ahead of the drain, so the drain's
-//               latency stays off the tensor pipe even when a chunk is one
-//               stage long (K-split plans).
+//               32x32b), chunk sums in registers, then the tile goes out
+//               through swizzled shared-memory boxes and TMA stores (where the
+//               boxes fit beside the ring: TMA_STORE) or straight from
+//               registers. The MMAs run up to NACC - 1 chunks ahead of the
+//               drain, so the drain's latency stays off the tensor pipe even
+//               when a chunk is one stage long (K-split plans).
 // Work units are (output tile, K slice) pairs; with several slices per tile,
 // each slice writes a partial and the last slice to arrive (per warp's rows
 // and columns) sums the partials in slice order into C, deterministically.
 //
 // Edges: the TMA boxes read zero outside the planes (M and K tails), the
-// planes are zero-padded in K and N, and the epilogue predicates its stores,
-// the counterpart of the reference's scratch-tile edge path (:539-558).
+// planes are zero-padded in K and N, and the epilogue's TMA store boxes are
+// clipped at C's extent (register stores are predicated), the counterpart of
+// the reference's scratch-tile edge path (:539-558).
 //
 // Every wait on an mbarrier is bounded; on timeout the kernel records
 // kErrTimeout in the device error word, stops issuing work, waits (bounded)
