@@ -527,16 +527,18 @@ def main() -> None:
     # Split mode: the one given, or the fastest on this device (picked during
     # warm-up, untimed; every mode meets the accuracy bar at this shape).
     if args.precision == "auto":
-        best = None
-        for name, pc in PREC.items():
-            fn, _, keep = mode_step(pc, dC)
+        # The modes are within a few per cent of each other at this shape:
+        # three rounds over all of them, each mode's best round decides.
+        steps = {name: mode_step(pc, dC) for name, pc in PREC.items()}
+        for fn, _, _ in steps.values():
             for _ in range(3):
                 fn()
-            t = timed(fn, 20)
-            if best is None or t < best[0]:
-                best = (t, name)
-            del keep
-        args.precision = best[1]
+        best_t = {name: float("inf") for name in steps}
+        for _ in range(3):
+            for name, (fn, _, _) in steps.items():
+                best_t[name] = min(best_t[name], timed(fn, 30))
+        args.precision = min(best_t, key=best_t.get)
+        del steps
     prec = 0 if args.precision == "fp32" else PREC[args.precision]
     if prec == 0:
         args.no_extras = True
