@@ -328,6 +328,31 @@ const char* maxmulsk_last_error_message(void);
 /* Library version, e.g. "0.1.0". */
 const char* maxmulsk_version(void);
 
+/* ----------------------------------------------------------------------------
+ * Phase timing: the counterpart of the reference's lab hooks
+ * (sme/support/lab_hooks.hpp:1-22, scopes in
+ * sme/v3/sme-1x4-acc-kcout.cpp:453-561) and of its per-phase timing breakdown
+ * (sme/support/test_sme.cpp:580-678). Off by default; on with
+ * MAXMULSK_PHASE_TIMING=1 in the environment or maxmulsk_phase_timing(1).
+ * While on, every call outside a CUDA graph capture records a CUDA event pair
+ * on its stream around each phase, and an NVTX range on the host thread:
+ *   "split"   operand planes of the split-precision path (pre-pass)
+ *   "gemm"    the GEMM kernel (SIMT or tcgen05)
+ *   "reduce"  the split-K reduction kernel of plans with 3 or more K slices
+ *   "grouped" one grouped batch (its CUDA graph)
+ *   "h2d" / "d2h"  the host entry points' copies (pipelined copies overlap)
+ * Up to 65536 phases are held between two reports; later ones are dropped.
+ * ------------------------------------------------------------------------- */
+void maxmulsk_phase_timing(int32_t on);
+
+/* Waits for the phases recorded since the last report and writes
+ * {"split": {"calls": n, "ms": t}, ...} (device milliseconds summed per phase;
+ * phases with no calls omitted) into buf, NUL-terminated, truncated to len
+ * bytes, and forgets them. Returns the length of the whole text, which never
+ * exceeds MAXMULSK_PHASE_REPORT_BYTES - 1. */
+#define MAXMULSK_PHASE_REPORT_BYTES 1024
+size_t maxmulsk_phase_report(char* buf, size_t len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -42,6 +42,7 @@ FP32_SCALAR = 1
 TC_SPLIT_INPUTS = 0
 TC_REUSE_PLANES = 1
 TC_FUSED_SPLIT = 2
+PHASE_REPORT_BYTES = 1024   # MAXMULSK_PHASE_REPORT_BYTES
 
 
 class MaxMulSKError(RuntimeError):
@@ -218,6 +219,20 @@ def last_error_message() -> str:
 
 def version() -> str:
     return lib().maxmulsk_version().decode()
+
+
+def phase_timing(on: bool = True) -> None:
+    """Turns phase timing on or off (maxmulsk_phase_timing)."""
+    lib().maxmulsk_phase_timing(1 if on else 0)
+
+
+def phase_report() -> dict:
+    """Device time per phase since the last report, {"gemm": {"calls": n, "ms": t}, ...}
+    (maxmulsk_phase_report); the recorded phases are then forgotten."""
+    import json
+    buf = ctypes.create_string_buffer(PHASE_REPORT_BYTES)
+    lib().maxmulsk_phase_report(buf, PHASE_REPORT_BYTES)
+    return json.loads(buf.value.decode())
 
 
 def check(status: int, where: str = "maxmulsk") -> None:

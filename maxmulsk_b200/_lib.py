@@ -98,6 +98,8 @@ _SIGNATURES: dict[str, tuple] = {
     "maxmulsk_status_string": (c_char_p, [c_int32]),
     "maxmulsk_last_error_message": (c_char_p, []),
     "maxmulsk_version": (c_char_p, []),
+    "maxmulsk_phase_timing": (None, [c_int32]),
+    "maxmulsk_phase_report": (c_size_t, [c_char_p, c_size_t]),
 }
 
 _lib: ctypes.CDLL | None = None

@@ -7,6 +7,7 @@
 
 #include "maxmulsk.h"
 #include "internal.hpp"
+#include "phase.hpp"
 #include "runtime.hpp"
 #include "tuning.hpp"
 
@@ -122,6 +123,10 @@ maxmulsk_status maxmulsk_sgemm_plan_static_dev(const float* dA, const float* dB,
     if (!plan) { mmsk::set_error_message("null plan"); return MAXMULSK_ERR_INVALID; }
     return mmsk::simt_run_static_scratch(dA, dB, dC, M, K, N, *plan, static_cast<cudaStream_t>(stream));
 }
+
+void maxmulsk_phase_timing(int32_t on) { mmsk::phase_set(on != 0); }
+
+size_t maxmulsk_phase_report(char* buf, size_t len) { return mmsk::phase_report(buf, len); }
 
 size_t maxmulsk_probe_split_bytes(size_t R, size_t C, int32_t precision, int32_t as_b) {
     if (!is_split_precision(precision)) return 0;

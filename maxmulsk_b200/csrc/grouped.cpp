@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "internal.hpp"
+#include "phase.hpp"
 #include "runtime.hpp"
 
 struct maxmulsk_grouped_s {
@@ -424,6 +425,7 @@ maxmulsk_status maxmulsk_grouped_create(const maxmulsk_problem* problems, size_t
 
 maxmulsk_status maxmulsk_grouped_launch(maxmulsk_grouped g, void* stream) {
     if (!g || !g->exec) return MAXMULSK_ERR_INVALID;
+    PhaseScope ps(kPhaseGrouped, static_cast<cudaStream_t>(stream));
     return cuda_status(cudaGraphLaunch(g->exec, static_cast<cudaStream_t>(stream)), "cudaGraphLaunch(grouped)");
 }
 

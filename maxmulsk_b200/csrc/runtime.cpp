@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "internal.hpp"
+#include "phase.hpp"
 
 namespace mmsk {
 
@@ -278,14 +279,20 @@ maxmulsk_status host_pipelined(HostStage& hs, const float* A, const float* B, fl
         return e;
     };
 
-    st = cuda_status(cudaMemcpyAsync(hs.dB, B, K * N * sizeof(float), cudaMemcpyHostToDevice, hs.h2d), "copy B");
+    {
+        PhaseScope ps(kPhaseH2D, hs.h2d);
+        st = cuda_status(cudaMemcpyAsync(hs.dB, B, K * N * sizeof(float), cudaMemcpyHostToDevice, hs.h2d), "copy B");
+    }
     if (st != MAXMULSK_OK) return fail(st);
     st = cuda_status(cudaEventRecord(hs.b_in, hs.h2d), "cudaEventRecord");
     if (st != MAXMULSK_OK) return fail(st);
     for (int i = 0; i < nblk; i++) {
         const size_t r0 = (size_t)i * rows, mb = std::min(rows, M - r0);
-        st = cuda_status(cudaMemcpyAsync(hs.dA + r0 * K, A + r0 * K, mb * K * sizeof(float), cudaMemcpyHostToDevice,
-                                         hs.h2d), "copy A block");
+        {
+            PhaseScope ps(kPhaseH2D, hs.h2d);
+            st = cuda_status(cudaMemcpyAsync(hs.dA + r0 * K, A + r0 * K, mb * K * sizeof(float),
+                                             cudaMemcpyHostToDevice, hs.h2d), "copy A block");
+        }
         if (st != MAXMULSK_OK) return fail(st);
         st = cuda_status(cudaEventRecord(hs.a_in[i], hs.h2d), "cudaEventRecord");
         if (st != MAXMULSK_OK) return fail(st);
@@ -299,7 +306,10 @@ maxmulsk_status host_pipelined(HostStage& hs, const float* A, const float* B, fl
         const size_t nb = split_one_bytes((int64_t)K, (int64_t)N, plan.precision, true);
         st = cuda_status(grow(&hs.dBp, &hs.capBp, (nb + sizeof(float) - 1) / sizeof(float)), "cudaMalloc(B planes)");
         if (st != MAXMULSK_OK) return fail(st);
-        st = cuda_status(split_one(hs.dB, (int64_t)K, (int64_t)N, plan.precision, true, hs.dBp, s), "split B");
+        {
+            PhaseScope ps(kPhaseSplit, s);
+            st = cuda_status(split_one(hs.dB, (int64_t)K, (int64_t)N, plan.precision, true, hs.dBp, s), "split B");
+        }
         if (st != MAXMULSK_OK) return fail(st);
         b_planes = hs.dBp;
     }
@@ -313,8 +323,11 @@ maxmulsk_status host_pipelined(HostStage& hs, const float* A, const float* B, fl
         if (st != MAXMULSK_OK) return fail(st);
         st = cuda_status(cudaStreamWaitEvent(hs.d2h, hs.c_done[i], 0), "cudaStreamWaitEvent");
         if (st != MAXMULSK_OK) return fail(st);
-        st = cuda_status(cudaMemcpyAsync(C + r0 * N, hs.dC + r0 * N, mb * N * sizeof(float), cudaMemcpyDeviceToHost,
-                                         hs.d2h), "copy C block");
+        {
+            PhaseScope ps(kPhaseD2H, hs.d2h);
+            st = cuda_status(cudaMemcpyAsync(C + r0 * N, hs.dC + r0 * N, mb * N * sizeof(float),
+                                             cudaMemcpyDeviceToHost, hs.d2h), "copy C block");
+        }
         if (st != MAXMULSK_OK) return fail(st);
     }
     st = cuda_status(cudaStreamSynchronize(hs.d2h), "cudaStreamSynchronize");
@@ -353,13 +366,19 @@ maxmulsk_status run_plan_host(const float* A, const float* B, float* C, size_t M
         return host_pipelined(hs, A, B, C, M, K, N, plan);
 
     cudaStream_t s = hs.stream;
-    st = cuda_status(cudaMemcpyAsync(hs.dA, A, M * K * sizeof(float), cudaMemcpyHostToDevice, s), "copy A");
-    if (st != MAXMULSK_OK) return st;
-    st = cuda_status(cudaMemcpyAsync(hs.dB, B, K * N * sizeof(float), cudaMemcpyHostToDevice, s), "copy B");
+    {
+        PhaseScope ps(kPhaseH2D, s);
+        st = cuda_status(cudaMemcpyAsync(hs.dA, A, M * K * sizeof(float), cudaMemcpyHostToDevice, s), "copy A");
+        if (st == MAXMULSK_OK)
+            st = cuda_status(cudaMemcpyAsync(hs.dB, B, K * N * sizeof(float), cudaMemcpyHostToDevice, s), "copy B");
+    }
     if (st != MAXMULSK_OK) return st;
     st = run_plan_managed(hs.dA, hs.dB, hs.dC, M, K, N, plan, s);
     if (st != MAXMULSK_OK) { cudaStreamSynchronize(s); return st; }
-    st = cuda_status(cudaMemcpyAsync(C, hs.dC, M * N * sizeof(float), cudaMemcpyDeviceToHost, s), "copy C");
+    {
+        PhaseScope ps(kPhaseD2H, s);
+        st = cuda_status(cudaMemcpyAsync(C, hs.dC, M * N * sizeof(float), cudaMemcpyDeviceToHost, s), "copy C");
+    }
     if (st != MAXMULSK_OK) { cudaStreamSynchronize(s); return st; }
     return stream_status(s);
 }

@@ -25,6 +25,7 @@
 #include <mutex>
 
 #include "internal.hpp"
+#include "phase.hpp"
 #include "runtime.hpp"
 #include "split_math.cuh"
 
@@ -333,12 +334,17 @@ cudaError_t launch_tile(const SimtArgs& args, int variant, cudaStream_t s) {
     const bool vec = (a.K % 4 == 0) && (a.N % 4 == 0) &&
                      ((uintptr_t)a.A % 16 == 0) && ((uintptr_t)a.B % 16 == 0) && ((uintptr_t)a.C % 16 == 0);
     const bool fused = (variant != MAXMULSK_FP32_SCALAR);
-    if (fused && vec) sgemm_simt_kernel<BM, BN, true, true><<<grid, kThreads, 0, s>>>(a);
-    else if (fused) sgemm_simt_kernel<BM, BN, true, false><<<grid, kThreads, 0, s>>>(a);
-    else if (vec) sgemm_simt_kernel<BM, BN, false, true><<<grid, kThreads, 0, s>>>(a);
-    else sgemm_simt_kernel<BM, BN, false, false><<<grid, kThreads, 0, s>>>(a);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e;
+    {
+        PhaseScope ps(kPhaseGemm, s);
+        if (fused && vec) sgemm_simt_kernel<BM, BN, true, true><<<grid, kThreads, 0, s>>>(a);
+        else if (fused) sgemm_simt_kernel<BM, BN, true, false><<<grid, kThreads, 0, s>>>(a);
+        else if (vec) sgemm_simt_kernel<BM, BN, false, true><<<grid, kThreads, 0, s>>>(a);
+        else sgemm_simt_kernel<BM, BN, false, false><<<grid, kThreads, 0, s>>>(a);
+        e = cudaGetLastError();
+    }
     if (e != cudaSuccess || !a.reduce_after) return e;
+    PhaseScope ps(kPhaseReduce, s);
     int64_t blocks = (a.M * a.N + 255) / 256;
     const int64_t cap = (int64_t)device_sm_count() * 8;
     if (cap > 0 && blocks > cap) blocks = cap;

@@ -58,6 +58,7 @@
 #include <tuple>
 
 #include "internal.hpp"
+#include "phase.hpp"
 #include "sm100.cuh"
 #include "split_math.cuh"
 
@@ -1397,9 +1398,13 @@ cudaError_t launch_cfg(const TcArgs& a, cudaStream_t s) {
     static std::atomic<uint64_t> smem_set{0};
     cudaError_t e = set_smem_once(tc_gemm_kernel<MODE, BN>, Cf::SMEM, smem_set);
     if (e != cudaSuccess) return e;
-    tc_gemm_kernel<MODE, BN><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, tmC, prm);
-    e = cudaGetLastError();
+    {
+        PhaseScope ps(kPhaseGemm, s);
+        tc_gemm_kernel<MODE, BN><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, tmC, prm);
+        e = cudaGetLastError();
+    }
     if (e != cudaSuccess || !prm.reduce_after) return e;
+    PhaseScope ps(kPhaseReduce, s);
     return launch_reduce<BN>(prm, s);
 }
 
@@ -1466,10 +1471,13 @@ cudaError_t launch_cfg_pair(const TcArgs& a, cudaStream_t s) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    e = cudaLaunchKernelEx(&cfg, tc_gemm_pair_kernel<MODE, BN>, tmA, tmB, tmC, prm);
-    if (e != cudaSuccess) return e;
-    e = cudaGetLastError();
+    {
+        PhaseScope ps(kPhaseGemm, s);
+        e = cudaLaunchKernelEx(&cfg, tc_gemm_pair_kernel<MODE, BN>, tmA, tmB, tmC, prm);
+        if (e == cudaSuccess) e = cudaGetLastError();
+    }
     if (e != cudaSuccess || !prm.reduce_after) return e;
+    PhaseScope ps(kPhaseReduce, s);
     return launch_reduce<BN>(prm, s);
 }
 
@@ -1520,9 +1528,13 @@ cudaError_t launch_fused(const TcArgs& a, cudaStream_t s) {
     cudaError_t e = set_smem_once(tc_fused_kernel<MODE, false>, Cf::SMEM, smem_set);
     if (e != cudaSuccess) return e;
     TcGroupArgs none{};
-    tc_fused_kernel<MODE, false><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, tmC, prm, none);
-    e = cudaGetLastError();
+    {
+        PhaseScope ps(kPhaseGemm, s);
+        tc_fused_kernel<MODE, false><<<(unsigned)sc.grid, Cf::THREADS, Cf::SMEM, s>>>(tmA, tmB, tmC, prm, none);
+        e = cudaGetLastError();
+    }
     if (e != cudaSuccess || !prm.reduce_after) return e;
+    PhaseScope ps(kPhaseReduce, s);
     return launch_reduce<BN>(prm, s);
 }
 
@@ -1629,6 +1641,7 @@ cudaError_t tc_launch(const TcArgs& a, cudaStream_t s) {
     }
     if (!a.reuse_planes) {
         // With B's planes supplied from outside only A is split here.
+        PhaseScope ps(kPhaseSplit, s);
         cudaError_t e = a.b_planes ? split_one(a.A, a.M, a.K, a.precision, false, a.planes, s)
                                    : split_launch(a.A, a.B, a.M, a.K, a.N, a.precision, a.planes, s);
         if (e != cudaSuccess) return e;

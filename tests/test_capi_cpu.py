@@ -108,3 +108,15 @@ def test_fused_split_plan_rules(built_lib):
                 mm.make_plan(mm.Precision.BF16X6, 128, 256, 1, mm.TC_FUSED_SPLIT),
                 mm.make_plan(mm.Precision.BF16X9, 256, 128, 1, mm.TC_FUSED_SPLIT)):
         assert mm.classify(256, 256, 256, bad) == mm.Status.ERR_UNSUPPORTED
+
+
+def test_phase_report_without_records(built_lib):
+    # Nothing recorded: the empty report and its length; the switch and the
+    # report touch no device when there is nothing to wait for.
+    buf = ctypes.create_string_buffer(64)
+    assert built_lib.maxmulsk_phase_report(buf, 64) == 2 and buf.value == b"{}"
+    built_lib.maxmulsk_phase_timing(1)
+    built_lib.maxmulsk_phase_timing(0)
+    assert mm.phase_report() == {}
+    small = ctypes.create_string_buffer(1)
+    assert built_lib.maxmulsk_phase_report(small, 1) == 2 and small.value == b""
