@@ -623,6 +623,17 @@ def main() -> None:
                           f"{' / 2 (TF32 rate)' if prec == 1 else ''} / {PRODUCTS[prec]} products; useful 2MNK flops",
             "gemm_ms": t_gemm * 1e3, "prepass_ms": max(0.0, (t_step - t_gemm) * 1e3),
         }
+        # ---- phase breakdown of the headline step (maxmulsk_phase_report: CUDA
+        # events around the split pre-pass and the GEMM; outside the timed region)
+        mm.phase_report()
+        mm.phase_timing(True)
+        for _ in range(20):
+            step_tc()
+        torch.cuda.synchronize(dev)
+        phases = mm.phase_report()
+        mm.phase_timing(False)
+        out["phases"] = {k: {"calls_per_step": v["calls"] / 20, "ms_per_step": v["ms"] / 20}
+                         for k, v in phases.items()}
         # ---- the FP32 SIMT kernel on the same inputs
         for _ in range(3):
             step_simt()
