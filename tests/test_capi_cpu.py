@@ -120,3 +120,22 @@ def test_phase_report_without_records(built_lib):
     assert mm.phase_report() == {}
     small = ctypes.create_string_buffer(1)
     assert built_lib.maxmulsk_phase_report(small, 1) == 2 and small.value == b""
+
+
+@pytest.mark.parametrize("compiler", [["gcc", "-std=c99", "-x", "c"], ["g++", "-std=c++17", "-x", "c++"]])
+def test_c_caller_compiles_links_and_runs(built_lib, tmp_path, compiler):
+    # A C (and a C++) caller of the header: it compiles with -Wall -Werror,
+    # links every entry point against the library and runs its host-only
+    # calls (no device work).
+    import os
+    here = os.path.dirname(os.path.abspath(__file__))
+    inc = os.path.join(os.path.dirname(here), "include")
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    exe = str(tmp_path / "c_abi_check")
+    cmd = compiler + ["-Wall", "-Wextra", "-Werror", "-I", inc, os.path.join(here, "c_abi_check.c"),
+                      "-x", "none", "-L", libdir, "-lmaxmulsk_b200", f"-Wl,-rpath,{libdir}", "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert r.stdout.startswith("c-abi ok")
