@@ -8,9 +8,11 @@ seed), the shape the speed target is stated on.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--size S] [--precision auto|fp32|tf32x3|bf16x6|bf16x9]
 
-Multi-GPU (torchrun, one rank per GPU): every rank multiplies its own M-row
-shard (a 4096 x 4096 block of A and the whole B); no collective touches the
-data path. Timing is on the device (CUDA events), max over ranks.
+Multi-GPU (one rank per GPU): under torchrun, or `--gpus N` alone, which
+starts the N ranks itself through torch.distributed.run. Every rank
+multiplies its own M-row shard (a 4096 x 4096 block of A and the whole B); no
+collective touches the data path. Timing is on the device (CUDA events), max
+over ranks; a line is printed only when the ranks started match --gpus.
 
 The reference arm (--impl reference) times the reference's own CPU GEMM,
 Utils::multiply_scalar (common/utils.hpp:50-61) compiled into oracle/_ref, on
@@ -77,6 +79,75 @@ def launches_per_step(plan, K: int) -> int:
     if mm.slice_count(K, plan.split_k) >= 3:
         n += 1
     return n
+
+
+# ----------------------------------------------------------------------------- ranks
+def launch_ranks(n: int) -> int:
+    """Runs this script again as n ranks, one process per GPU, under
+    torch.distributed.run on 127.0.0.1 (the form `bench.py --gpus n` takes
+    when no launcher set WORLD_SIZE); returns their exit status. NCCL's log
+    stays on (NCCL_DEBUG=INFO unless set), so the communicator's ranks show."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    env = dict(os.environ)
+    env.setdefault("NCCL_DEBUG", "INFO")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd, env=env).returncode
+
+
+class Ranks:
+    """One rank per GPU (RANK / WORLD_SIZE / LOCAL_RANK from the launcher):
+    barriers and the max over ranks of a per-rank time. Nothing on the data
+    path is exchanged: each rank multiplies its own shard."""
+
+    def __init__(self, backend: str = "nccl", device=None):
+        self.rank = env_int("RANK", 0)
+        self.world = env_int("WORLD_SIZE", 1)
+        self.local = env_int("LOCAL_RANK", 0)
+        self.backend = backend
+        self.device = device
+        if self.world > 1:
+            from datetime import timedelta
+
+            import torch.distributed as dist
+            kw = {"device_id": device} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=timedelta(seconds=120), **kw)
+
+    def barrier(self) -> None:
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, x: float) -> float:
+        from maxmulsk_b200 import shard
+        return shard.max_over_ranks(x, self.device if self.backend == "nccl" else None)
+
+    def timed(self, fn, steps: int, start, stop) -> float:
+        """Seconds per step of fn, the max over ranks: barrier, t0 = start(),
+        `steps` calls, stop(t0) -> seconds, barrier."""
+        self.barrier()
+        t0 = start()
+        for _ in range(steps):
+            fn()
+        secs = stop(t0)
+        self.barrier()
+        return self.max(secs / steps)
+
+    def close(self) -> None:
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+def check_world(gpus: int, world: int) -> None:
+    """A line's n_gpus must be what --gpus asked for."""
+    if world != gpus:
+        print(f"bench.py: --gpus {gpus} but the launcher started {world} rank(s); no line printed",
+              file=sys.stderr)
+        sys.exit(2)
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -278,13 +349,9 @@ def run_tables(args) -> None:
             mm.check(mm.sgemm_plan_dev(dA, dB, dC, M, K, N, plan, wp, nb), "plan")
         return fn, ws
 
-    def errors(dA, dB, dC, M, K, N):
-        A64, B64 = dA.view(M, K).double(), dB.view(K, N).double()
-        C64 = A64 @ B64
-        d = (dC.view(M, N).double() - C64).abs()
-        floor = (A64.abs() @ B64.abs()) * 2.0 ** -24
-        nw = float(torch.linalg.norm(d) / (torch.linalg.norm(A64) * torch.linalg.norm(B64)))
-        return nw, float((d / torch.maximum(C64.abs(), floor)).max())
+    def errors(chk, dC):
+        e = chk.errors(dC)
+        return e["normwise"], e["max_rel"]
 
     def emit(d):
         print(json.dumps(d), flush=True)
@@ -302,6 +369,7 @@ def run_tables(args) -> None:
             else:
                 A = datagen.uniform(M * K, 31); B = datagen.uniform(K * N, 32)
             dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+            chk = mm.Fp64Check(dA, dB, M, K, N)         # the library's FP64 check product
             flops = 2.0 * M * N * K
             bytes_min = 4.0 * (M * K + K * N + M * N)
             # The plain FP32 kernel: one FMA chain per output (split_k = 1; the
@@ -311,7 +379,7 @@ def run_tables(args) -> None:
             dCp = torch.empty(M * N, device="cuda")
             fn_p, ws_p = run_plan(dA, dB, dCp, M, K, N, mm.make_plan(0, 128, 128, 1))
             fn_p()
-            plain_err, _ = errors(dA, dB, dCp, M, K, N)
+            plain_err, _ = errors(chk, dCp)
             del ws_p, dCp
             simt_err = None
             for name, pc in kernels:
@@ -320,7 +388,7 @@ def run_tables(args) -> None:
                 fn, ws = run_plan(dA, dB, dC, M, K, N, plan)
                 reps = int(max(3, min(200, 2e10 / flops)))
                 t = graph_time(torch, fn, reps)
-                nw, mr = errors(dA, dB, dC, M, K, N)
+                nw, mr = errors(chk, dC)
                 if pc == 0:
                     simt_err = nw
                 peak = fp32_peak if pc == 0 else peaks["bf16_tflops"] / (2.0 if pc == 1 else 1.0) / PRODUCTS[pc]
@@ -393,9 +461,7 @@ def run_tables(args) -> None:
         nw = []
         for i in np.random.default_rng(0).choice(len(shapes), 16, replace=False):
             a, b, c, M, K, N = probs[i]
-            ref = a.view(M, K).double() @ b.view(K, N).double()
-            nw.append(float(torch.linalg.norm(c.view(M, N).double() - ref) /
-                            (torch.linalg.norm(a.double()) * torch.linalg.norm(b.double()))))
+            nw.append(mm.Fp64Check(a, b, M, K, N, with_abs=False).errors(c)["normwise"])
         emit({"workload": "grouped", "precision": name, "problems": len(shapes), "gflop": flops / 1e9,
               "units": tunits, "fp32_fallback_problems": sum(1 for M, K, N in shapes if N % 4),
               "a_repacked_problems": sum(1 for M, K, N in shapes if K % 4 and not N % 4),
@@ -429,6 +495,9 @@ def main() -> None:
                     help="square4096 (default, one JSON line) or a per-cell table of the other configurations")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        sys.exit(launch_ranks(args.gpus))
+    check_world(args.gpus, env_int("WORLD_SIZE", 1))
 
     if args.impl == "reference":
         run_reference(args)
@@ -439,19 +508,15 @@ def main() -> None:
 
     import numpy as np
     import torch
-    import torch.distributed as dist
 
     import maxmulsk_b200 as mm
     from maxmulsk_b200 import datagen
 
-    rank = env_int("RANK", 0)
-    world = env_int("WORLD_SIZE", 1)
     local = env_int("LOCAL_RANK", 0)
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    ranks = Ranks("nccl", dev)
+    rank, world = ranks.rank, ranks.world
 
     S = args.size
     M = K = N = S
@@ -471,30 +536,23 @@ def main() -> None:
     dCs = torch.empty((M, N), dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = ranks.barrier
+    max_over_ranks = ranks.max
 
     def timed(fn, steps: int) -> float:
-        """Seconds per step: CUDA events on the launching stream, synchronize on both sides."""
-        barrier()
-        torch.cuda.synchronize(dev)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(steps):
-            fn()
-        e1.record(stream)
-        torch.cuda.synchronize(dev)
-        barrier()
-        return max_over_ranks(e0.elapsed_time(e1) / 1e3 / steps)
+        """Seconds per step: CUDA events on the launching stream, synchronize
+        on both sides, barriers around, the max over ranks."""
+        def start():
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            return e0, e1
+
+        def stop(ev):
+            ev[1].record(stream)
+            torch.cuda.synchronize(dev)
+            return ev[0].elapsed_time(ev[1]) / 1e3
+        return ranks.timed(fn, steps, start, stop)
 
     def mode_step(pc: int, out):
         mp = mm.choose(M, K, N, pc)
@@ -659,22 +717,18 @@ def main() -> None:
             del mws
         out["speedup_vs_simt"] = (flops / t_step) / (flops / t_simt)
         out["speedup_vs_simt_gemm_only"] = t_simt / t_gemm
-        # ---- FP64-measured error of both kernels (cuBLAS DGEMM as the FP64 product, outside timing);
+        # ---- FP64-measured error of both kernels (the library's FP64 check product, outside timing);
         # the plain FP32 kernel (one FMA chain per output, split_k 1) is the error bar
         dCp = torch.empty((M, N), dtype=torch.float32, device=dev)
         mm.check(mm.sgemm_plan_dev(dA, dB, dCp, M, K, N, mm.make_plan(0, 128, 128, 1), None, 0, stream), "plain")
         if rank == 0:
-            with torch.no_grad():
-                A64, B64 = dA.double(), dB.double()
-                C64 = A64 @ B64
-                floor = (A64.abs() @ B64.abs()) * 2.0 ** -24
-                nab = torch.linalg.norm(A64) * torch.linalg.norm(B64)
-                errs = {}
-                for name, Cx in [("tc", dC), ("simt", dCs), ("plain_fp32", dCp)] + [(k, v["_C"]) for k, v in modes.items()]:
-                    d = (Cx.double() - C64).abs()
-                    errs[name] = {"normwise": float(torch.linalg.norm(d) / nab),
-                                  "max_rel": float((d / torch.maximum(C64.abs(), floor)).max())}
-                del A64, B64, C64, floor
+            # the library's FP64 check product and device error reduction
+            chk = mm.Fp64Check(dA, dB, M, K, N, stream=stream)
+            errs = {}
+            for name, Cx in [("tc", dC), ("simt", dCs), ("plain_fp32", dCp)] + [(k, v["_C"]) for k, v in modes.items()]:
+                e = chk.errors(Cx, stream=stream)
+                errs[name] = {"normwise": e["normwise"], "max_rel": e["max_rel"]}
+            del chk
             errs["tc_over_simt_normwise"] = errs["tc"]["normwise"] / errs["simt"]["normwise"]
             out["fp64_error"] = {"tc": errs["tc"], "simt": errs["simt"], "plain_fp32": errs["plain_fp32"],
                                  "tc_over_simt_normwise": errs["tc_over_simt_normwise"],
@@ -708,8 +762,7 @@ def main() -> None:
 
     if rank == 0:
         print(json.dumps(out), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
 
 
 if __name__ == "__main__":

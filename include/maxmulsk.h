@@ -46,9 +46,13 @@ typedef enum {
  * ------------------------------------------------------------------------- */
 
 /* Replaces capi/maxmulsk.h:32-33 (SMEKernels1x4AccKcOut). The plan comes from
- * the tuning picker (tuning database, else the learned cost model, else the
- * shape rule), FP32 SIMT precision; MAXMULSK_CONFIG overrides it. Unlike the
- * reference's v3, allocation failure is reported (MAXMULSK_ERR_ALLOC). */
+ * the tuning picker, FP32 SIMT precision; MAXMULSK_CONFIG overrides it. The
+ * picker: the tuning database; else, when the learned cost model cannot be
+ * trusted for the shape (see maxmulsk_picker_doubt), an exhaustive search of
+ * the candidates on the call's own operands (device copies of them for host
+ * pointers; never inside a stream capture) whose winner enters the database;
+ * else the learned model; else the shape rule. Unlike the reference's v3,
+ * allocation failure is reported (MAXMULSK_ERR_ALLOC). */
 maxmulsk_status maxmulsk_sgemm_v3(const float* A, const float* B, float* C,
                                   size_t M, size_t K, size_t N);
 
@@ -128,9 +132,22 @@ typedef struct {
 maxmulsk_status maxmulsk_classify(size_t M, size_t K, size_t N, const maxmulsk_plan* plan);
 
 /* The picker behind maxmulsk_sgemm_v3 for a given precision (the analog of
- * MaxMulSK::tuning::select, sme/support/gemm_tuning.cpp:96-100). */
+ * MaxMulSK::tuning::select, sme/support/gemm_tuning.cpp:96-100), as a query:
+ * MAXMULSK_CONFIG, the tuning database, the learned model, the rule. It has
+ * no operands, so it never searches; after a GEMM call on the shape ran the
+ * exhaustive fallback, it returns that call's plan (now in the database). */
 maxmulsk_status maxmulsk_choose(size_t M, size_t K, size_t N, int32_t precision,
                                 maxmulsk_plan* out);
+
+/* Why the GEMM entry points would run the exhaustive search for this shape
+ * and precision instead of trusting the learned model: "no learned model",
+ * "shape outside the trained range" (M, N or K above 16384), "close call"
+ * (its two best candidates predicted within MAXMULSK_AUTOTUNE_MARGIN, default
+ * 0.005 in ln-time). NULL when the tuning database or the model decides, for
+ * BF16X9 (not searched), or with MAXMULSK_AUTOTUNE=0 (fallback off). The
+ * counterpart in the reference is the MAXMULSK_BLOCKING sweep override
+ * (sme/support/gemm_tuning.cpp:66-78). */
+const char* maxmulsk_picker_doubt(size_t M, size_t K, size_t N, int32_t precision);
 
 /* The fixed shape rule behind maxmulsk_sgemm_v4 (the analog of
  * SMEKernels1x4V4C::choose, sme/v4/sme-1x4-v4c-dispatch.cpp:17-22). */
@@ -158,7 +175,9 @@ maxmulsk_status maxmulsk_sgemm_plan(const float* A, const float* B, float* C,
 
 /* Split-precision tensor-core GEMM, selected explicitly (the plain names stay
  * FP32 SIMT). precision is one of MAXMULSK_PREC_3XTF32 / _BF16X6 / _BF16X9, or
- * MAXMULSK_PREC_SPLIT_AUTO to let the picker choose the split count. */
+ * MAXMULSK_PREC_SPLIT_AUTO to let the picker choose the split count. The
+ * plan comes from the picker as for maxmulsk_sgemm_v3 (exhaustive fallback
+ * included); MAXMULSK_CONFIG overrides it when its precision is the one asked. */
 maxmulsk_status maxmulsk_sgemm_split(const float* A, const float* B, float* C,
                                      size_t M, size_t K, size_t N, int32_t precision);
 maxmulsk_status maxmulsk_sgemm_split_dev(const float* dA, const float* dB, float* dC,
@@ -309,6 +328,44 @@ maxmulsk_status maxmulsk_mlp_predict_dev(const float* params, const float* X, co
 maxmulsk_status maxmulsk_sgemm_plan_static_dev(const float* dA, const float* dB, float* dC,
                                                size_t M, size_t K, size_t N,
                                                const maxmulsk_plan* plan, void* stream);
+
+/* ----------------------------------------------------------------------------
+ * FP64 checking (not on the product path: no GEMM entry point calls these).
+ * The GPU form of the reference's FP64 checks (every library compared with an
+ * FP64 product before timing, docs/BENCHMARKS.md:112-120 and :395-399) and of
+ * its checker Utils::check_correctness (common/utils.hpp:24-48), for products
+ * too large for a CPU loop in a test (4096^3, K = 32768, grouped batches).
+ * ------------------------------------------------------------------------- */
+
+/* C64[i][j] = sum_k (double)A[i][k] * (double)B[k][j], one fused multiply-add
+ * chain per output over k in increasing order from +0 -- bit for bit the
+ * sequential CPU loop (the product of two floats is exact in double). With
+ * dCabs non-NULL, also Cabs[i][j] = sum_k |A[i][k]| |B[k][j]| the same way.
+ * M x N doubles each, row-major. Asynchronous on `stream`. */
+maxmulsk_status maxmulsk_check_dgemm_dev(const float* dA, const float* dB, double* dC64, double* dCabs,
+                                         size_t M, size_t K, size_t N, void* stream);
+
+/* Error measures of an FP32 result C against C64. */
+typedef struct {
+    double normwise;   /* ||C - C64||_F / (||A||_F ||B||_F)                     */
+    double max_rel;    /* max |C - C64| / max(|C64|, 2^-24 Cabs), Cabs = 0 when
+                          no dCabs is given                                     */
+    double rel_frob;   /* ||C - C64||_F / ||C64||_F                             */
+    double max_abs;    /* max |C - C64|                                         */
+    double norm_a, norm_b, norm_diff, norm_c64;   /* the Frobenius norms used   */
+} maxmulsk_error_report;
+
+/* Bytes of device work memory maxmulsk_check_errors_dev needs (8-byte aligned). */
+size_t maxmulsk_check_errors_work_bytes(void);
+
+/* Computes the report with a deterministic two-pass reduction on the device
+ * (a fixed number of blocks, each summing a fixed subset in a fixed order,
+ * then the block results added in block order), waits for `stream` and writes
+ * it to *out (host memory). dCabs may be NULL. */
+maxmulsk_status maxmulsk_check_errors_dev(const float* dC, const double* dC64, const double* dCabs,
+                                          const float* dA, const float* dB, size_t M, size_t K, size_t N,
+                                          void* work, size_t work_bytes, maxmulsk_error_report* out,
+                                          void* stream);
 
 /* ----------------------------------------------------------------------------
  * Status, errors, device properties.

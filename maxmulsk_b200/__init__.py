@@ -15,7 +15,7 @@ import enum
 from typing import Any
 
 from . import _lib
-from ._lib import Plan, Problem
+from ._lib import ErrorReport, Plan, Problem
 
 __version__ = "0.1.0"
 
@@ -178,6 +178,13 @@ def choose(M: int, K: int, N: int, precision: int = Precision.FP32) -> Plan:
     return p
 
 
+def picker_doubt(M: int, K: int, N: int, precision: int = Precision.FP32) -> str | None:
+    """Why the GEMM entry points would search exhaustively for this shape
+    instead of trusting the learned model (maxmulsk_picker_doubt), or None."""
+    r = lib().maxmulsk_picker_doubt(M, K, N, int(precision))
+    return r.decode() if r else None
+
+
 def choose_rule(M: int, K: int, N: int, precision: int = Precision.FP32) -> Plan:
     p = Plan()
     st = lib().maxmulsk_choose_rule(M, K, N, int(precision), ctypes.byref(p))
@@ -233,6 +240,49 @@ def phase_report() -> dict:
     buf = ctypes.create_string_buffer(PHASE_REPORT_BYTES)
     lib().maxmulsk_phase_report(buf, PHASE_REPORT_BYTES)
     return json.loads(buf.value.decode())
+
+
+# --------------------------------------------------------------------------- FP64 checking
+def check_dgemm_dev(dA, dB, dC64, dCabs, M: int, K: int, N: int, stream=None) -> Status:
+    """C64 = A*B in FP64 on the device (and |A||B| when dCabs is given):
+    maxmulsk_check_dgemm_dev. dC64 / dCabs: float64 CUDA tensors or pointers."""
+    def ptr(x):
+        return None if x is None else (x if isinstance(x, int) else x.data_ptr())
+    return Status(lib().maxmulsk_check_dgemm_dev(_dev_ptr(dA, M * K, "A"), _dev_ptr(dB, K * N, "B"), ptr(dC64),
+                                                 ptr(dCabs), M, K, N, _stream_ptr(stream)))
+
+
+def check_errors_dev(dC, dC64, dCabs, dA, dB, M: int, K: int, N: int, stream=None) -> dict:
+    """Error measures of an FP32 result against C64 (maxmulsk_check_errors_dev):
+    {"normwise", "max_rel", "rel_frob", "max_abs", "norm_a", ...}."""
+    import torch
+
+    def ptr(x):
+        return None if x is None else (x if isinstance(x, int) else x.data_ptr())
+    nb = int(lib().maxmulsk_check_errors_work_bytes())
+    work = torch.empty(nb // 8 + 1, dtype=torch.float64, device="cuda")
+    rep = ErrorReport()
+    st = lib().maxmulsk_check_errors_dev(_dev_ptr(dC, M * N, "C"), ptr(dC64), ptr(dCabs), _dev_ptr(dA, M * K, "A"),
+                                         _dev_ptr(dB, K * N, "B"), M, K, N, work.data_ptr(), nb, ctypes.byref(rep),
+                                         _stream_ptr(stream))
+    check(st, "maxmulsk_check_errors_dev")
+    return rep.as_dict()
+
+
+class Fp64Check:
+    """FP64 truth of one product on the device, computed once, against which
+    several FP32 results are measured (the GPU form of the reference's FP64
+    checks). dA, dB: float32 CUDA tensors holding A (M x K) and B (K x N)."""
+
+    def __init__(self, dA, dB, M: int, K: int, N: int, with_abs: bool = True, stream=None):
+        import torch
+        self.dA, self.dB, self.M, self.K, self.N = dA, dB, M, K, N
+        self.c64 = torch.empty(M * N, dtype=torch.float64, device="cuda")
+        self.cabs = torch.empty(M * N, dtype=torch.float64, device="cuda") if with_abs else None
+        check(check_dgemm_dev(dA, dB, self.c64, self.cabs, M, K, N, stream), "maxmulsk_check_dgemm_dev")
+
+    def errors(self, dC, stream=None) -> dict:
+        return check_errors_dev(dC, self.c64, self.cabs, self.dA, self.dB, self.M, self.K, self.N, stream)
 
 
 def check(status: int, where: str = "maxmulsk") -> None:
@@ -323,6 +373,7 @@ __all__ = [
     "MaxMulSKError",
     "sgemm_v3", "sgemm_v4", "sgemm_plan", "sgemm_split",
     "sgemm_v3_dev", "sgemm_v4_dev", "sgemm_plan_dev", "sgemm_split_dev",
-    "make_plan", "classify", "choose", "choose_rule", "workspace_bytes", "slice_len", "slice_count",
+    "make_plan", "classify", "choose", "picker_doubt", "choose_rule", "workspace_bytes", "slice_len", "slice_count",
     "stream_status", "status_string", "last_error_message", "version", "check", "matmul", "lib", "Grouped",
+    "ErrorReport", "check_dgemm_dev", "check_errors_dev", "Fp64Check",
 ]

@@ -46,6 +46,24 @@ class Problem(ctypes.Structure):
     ]
 
 
+class ErrorReport(ctypes.Structure):
+    """maxmulsk_error_report: error measures of an FP32 result against FP64."""
+
+    _fields_ = [
+        ("normwise", ctypes.c_double),
+        ("max_rel", ctypes.c_double),
+        ("rel_frob", ctypes.c_double),
+        ("max_abs", ctypes.c_double),
+        ("norm_a", ctypes.c_double),
+        ("norm_b", ctypes.c_double),
+        ("norm_diff", ctypes.c_double),
+        ("norm_c64", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: float(getattr(self, name)) for name, _ in self._fields_}
+
+
 # name -> (restype, argtypes)
 _SIGNATURES: dict[str, tuple] = {
     "maxmulsk_sgemm_v3": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t]),
@@ -54,6 +72,7 @@ _SIGNATURES: dict[str, tuple] = {
     "maxmulsk_sgemm_v4_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t, c_void_p]),
     "maxmulsk_classify": (c_int32, [c_size_t, c_size_t, c_size_t, POINTER(Plan)]),
     "maxmulsk_choose": (c_int32, [c_size_t, c_size_t, c_size_t, c_int32, POINTER(Plan)]),
+    "maxmulsk_picker_doubt": (c_char_p, [c_size_t, c_size_t, c_size_t, c_int32]),
     "maxmulsk_choose_rule": (c_int32, [c_size_t, c_size_t, c_size_t, c_int32, POINTER(Plan)]),
     "maxmulsk_workspace_bytes": (c_size_t, [c_size_t, c_size_t, c_size_t, POINTER(Plan)]),
     "maxmulsk_sgemm_plan_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t,
@@ -94,6 +113,11 @@ _SIGNATURES: dict[str, tuple] = {
     "maxmulsk_probe_split_bytes": (c_size_t, [c_size_t, c_size_t, c_int32, c_int32]),
     "maxmulsk_probe_split_dev": (c_int32, [c_void_p, c_size_t, c_size_t, c_int32, c_int32, c_void_p, c_void_p]),
     "maxmulsk_probe_timeout_dev": (c_int32, [ctypes.c_int64, c_void_p]),
+    "maxmulsk_check_dgemm_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_size_t, c_size_t,
+                                           c_void_p]),
+    "maxmulsk_check_errors_work_bytes": (c_size_t, []),
+    "maxmulsk_check_errors_dev": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_size_t,
+                                            c_size_t, c_void_p, c_size_t, POINTER(ErrorReport), c_void_p]),
     "maxmulsk_stream_status": (c_int32, [c_void_p]),
     "maxmulsk_status_string": (c_char_p, [c_int32]),
     "maxmulsk_last_error_message": (c_char_p, []),
@@ -142,4 +166,4 @@ def exported_symbols() -> list[str]:
     return names
 
 
-__all__ = ["Plan", "Problem", "load", "exported_symbols", "LIB_PATH", "c_float"]
+__all__ = ["Plan", "Problem", "ErrorReport", "load", "exported_symbols", "LIB_PATH", "c_float"]

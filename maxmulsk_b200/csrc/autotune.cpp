@@ -14,6 +14,7 @@
 
 #include "internal.hpp"
 #include "mlp.hpp"
+#include "phase.hpp"
 #include "runtime.hpp"
 #include "tuning.hpp"
 
@@ -72,6 +73,7 @@ maxmulsk_status time_plan(const float* dA, const float* dB, float* dC, size_t M,
         if (st != MAXMULSK_OK) return st;
     }
     cudaStream_t s = t_tune.s;
+    PhaseMute mute;                                  // timing runs are not the caller's phases
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -123,6 +125,37 @@ maxmulsk_status time_plan(const float* dA, const float* dB, float* dC, size_t M,
 }
 
 }  // namespace
+
+void autotune_fallback(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N, int precision,
+                       cudaStream_t s) {
+    if (M == 0 || N == 0 || K == 0 || !dA || !dB || !dC) return;
+    if (!autotune_fallback_enabled() || !picker_doubt(M, K, N, precision)) return;
+    // Never inside a stream capture: the search synchronises and times.
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) { cudaGetLastError(); return; }
+    if (cs != cudaStreamCaptureStatusNone) return;
+    // Workspace for every candidate the learned model would also consider
+    // (split-K scratch up to 64 MiB + 4x the operand bytes).
+    const int cls = precision == MAXMULSK_PREC_FP32 ? 0 : 1;
+    maxmulsk_plan cands[MAXMULSK_MLP_OUTPUTS];
+    const int n = candidate_plans(cls, cands, MAXMULSK_MLP_OUTPUTS);
+    const size_t cap = (64u << 20) + 4 * sizeof(float) * (M * K + K * N + M * N);
+    size_t need = 0;
+    for (int i = 0; i < n; i++) {
+        if (classify_plan(M, K, N, &cands[i]) != MAXMULSK_OK) continue;
+        const size_t w = workspace_bytes(M, K, N, cands[i]);
+        if (w <= cap && w > need) need = w;
+    }
+    maxmulsk_status st = MAXMULSK_OK;
+    size_t ws_bytes = 0;
+    void* ws = need ? managed_workspace(s, need, &ws_bytes, &st) : nullptr;
+    if (need && !ws) return;
+    maxmulsk_plan best;
+    float us = 0.f;
+    st = maxmulsk_autotune_dev(dA, dB, dC, M, K, N, precision, ws, ws_bytes, &best, &us, s);
+    (void)st;   // on failure the picker keeps to the model or the rule
+}
+
 }  // namespace mmsk
 
 using namespace mmsk;

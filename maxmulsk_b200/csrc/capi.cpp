@@ -15,10 +15,23 @@ namespace {
 
 int sms_now() { return mmsk::device_sm_count(); }
 
-// v3: the picker (database, model, rule), FP32 SIMT; MAXMULSK_CONFIG wins.
-maxmulsk_plan plan_v3(size_t M, size_t K, size_t N) {
+// v3: the picker, FP32 SIMT; MAXMULSK_CONFIG wins. The picker: the tuning
+// database, else -- when the learned model cannot be trusted for the shape
+// (mmsk::picker_doubt) -- an exhaustive search on the call's own operands
+// whose winner enters the database, else the model, else the rule. The
+// search runs on device operands (dA, dB given, C overwritten), or, for host
+// pointers, on device copies of A and B.
+maxmulsk_plan plan_v3_host(const float* A, const float* B, size_t M, size_t K, size_t N) {
     maxmulsk_plan p;
     if (mmsk::parse_config_env(p)) return p;
+    mmsk::autotune_fallback_host(A, B, M, K, N, MAXMULSK_PREC_FP32);
+    return mmsk::choose_tuned(M, K, N, MAXMULSK_PREC_FP32, sms_now());
+}
+maxmulsk_plan plan_v3_dev(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
+                          cudaStream_t s) {
+    maxmulsk_plan p;
+    if (mmsk::parse_config_env(p)) return p;
+    mmsk::autotune_fallback(dA, dB, dC, M, K, N, MAXMULSK_PREC_FP32, s);
     return mmsk::choose_tuned(M, K, N, MAXMULSK_PREC_FP32, sms_now());
 }
 
@@ -32,9 +45,17 @@ bool is_split_precision(int32_t prec) {
            prec == MAXMULSK_PREC_SPLIT_AUTO;
 }
 
-maxmulsk_plan plan_split(size_t M, size_t K, size_t N, int32_t prec) {
+maxmulsk_plan plan_split_host(const float* A, const float* B, size_t M, size_t K, size_t N, int32_t prec) {
     maxmulsk_plan p;
     if (mmsk::parse_config_env(p) && p.precision == prec) return p;
+    mmsk::autotune_fallback_host(A, B, M, K, N, prec);
+    return mmsk::choose_tuned(M, K, N, prec, sms_now());
+}
+maxmulsk_plan plan_split_dev(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N, int32_t prec,
+                             cudaStream_t s) {
+    maxmulsk_plan p;
+    if (mmsk::parse_config_env(p) && p.precision == prec) return p;
+    mmsk::autotune_fallback(dA, dB, dC, M, K, N, prec, s);
     return mmsk::choose_tuned(M, K, N, prec, sms_now());
 }
 
@@ -44,7 +65,7 @@ extern "C" {
 
 maxmulsk_status maxmulsk_sgemm_v3(const float* A, const float* B, float* C, size_t M, size_t K, size_t N) {
     if (M == 0 || N == 0) return MAXMULSK_OK;
-    return mmsk::run_plan_host(A, B, C, M, K, N, plan_v3(M, K, N));
+    return mmsk::run_plan_host(A, B, C, M, K, N, plan_v3_host(A, B, M, K, N));
 }
 
 maxmulsk_status maxmulsk_sgemm_v4(const float* A, const float* B, float* C, size_t M, size_t K, size_t N) {
@@ -55,7 +76,8 @@ maxmulsk_status maxmulsk_sgemm_v4(const float* A, const float* B, float* C, size
 maxmulsk_status maxmulsk_sgemm_v3_dev(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
                                       void* stream) {
     if (M == 0 || N == 0) return MAXMULSK_OK;
-    return mmsk::run_plan_managed(dA, dB, dC, M, K, N, plan_v3(M, K, N), static_cast<cudaStream_t>(stream));
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    return mmsk::run_plan_managed(dA, dB, dC, M, K, N, plan_v3_dev(dA, dB, dC, M, K, N, s), s);
 }
 
 maxmulsk_status maxmulsk_sgemm_v4_dev(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
@@ -75,6 +97,12 @@ maxmulsk_status maxmulsk_choose(size_t M, size_t K, size_t N, int32_t precision,
     if (mmsk::parse_config_env(p) && p.precision == precision) { *out = p; return MAXMULSK_OK; }
     *out = mmsk::choose_tuned(M, K, N, precision, sms_now());
     return MAXMULSK_OK;
+}
+
+const char* maxmulsk_picker_doubt(size_t M, size_t K, size_t N, int32_t precision) {
+    if (precision != MAXMULSK_PREC_FP32 && !is_split_precision(precision)) return nullptr;
+    if (!mmsk::autotune_fallback_enabled()) return nullptr;
+    return mmsk::picker_doubt(M, K, N, precision);
 }
 
 maxmulsk_status maxmulsk_choose_rule(size_t M, size_t K, size_t N, int32_t precision, maxmulsk_plan* out) {
@@ -107,15 +135,15 @@ maxmulsk_status maxmulsk_sgemm_split(const float* A, const float* B, float* C, s
                                      int32_t precision) {
     if (!is_split_precision(precision)) return MAXMULSK_ERR_UNSUPPORTED;
     if (M == 0 || N == 0) return MAXMULSK_OK;
-    return mmsk::run_plan_host(A, B, C, M, K, N, plan_split(M, K, N, precision));
+    return mmsk::run_plan_host(A, B, C, M, K, N, plan_split_host(A, B, M, K, N, precision));
 }
 
 maxmulsk_status maxmulsk_sgemm_split_dev(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
                                          int32_t precision, void* stream) {
     if (!is_split_precision(precision)) return MAXMULSK_ERR_UNSUPPORTED;
     if (M == 0 || N == 0) return MAXMULSK_OK;
-    return mmsk::run_plan_managed(dA, dB, dC, M, K, N, plan_split(M, K, N, precision),
-                                  static_cast<cudaStream_t>(stream));
+    const cudaStream_t s = static_cast<cudaStream_t>(stream);
+    return mmsk::run_plan_managed(dA, dB, dC, M, K, N, plan_split_dev(dA, dB, dC, M, K, N, precision, s), s);
 }
 
 maxmulsk_status maxmulsk_sgemm_plan_static_dev(const float* dA, const float* dB, float* dC, size_t M, size_t K,

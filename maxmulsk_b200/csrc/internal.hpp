@@ -60,6 +60,12 @@ struct GroupUnit {
 };
 cudaError_t simt_grouped_launch(const GroupProblem* probs, const GroupUnit* units, int nunits, unsigned* next,
                                 int tile_m, int tile_n, int variant, int grid, cudaStream_t s);
+// Runs an FP32 plan whose split-K scratch (counters, then partials) is at
+// `scratch` (>= simt_workspace_bytes; may be null without a K split): lays it
+// out, clears the counters on `s`, launches. Both the workspace entry and the
+// static-scratch entry go through here.
+maxmulsk_status simt_run(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
+                         const maxmulsk_plan& plan, void* scratch, size_t scratch_bytes, cudaStream_t s);
 // The SIMT plan with its split-K scratch in a static device array (no allocation).
 maxmulsk_status simt_run_static_scratch(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
                                         const maxmulsk_plan& plan, cudaStream_t s);

@@ -236,7 +236,7 @@ bool mlp_predict_host(size_t M, size_t K, size_t N, int cls, float* y) {
     return true;
 }
 
-bool mlp_predict_plan(size_t M, size_t K, size_t N, int precision, maxmulsk_plan* out) {
+bool mlp_predict_plan(size_t M, size_t K, size_t N, int precision, maxmulsk_plan* out, float* margin) {
     const int cls = (precision == MAXMULSK_PREC_FP32) ? 0 : 1;
     if (precision == MAXMULSK_PREC_BF16X9) return false;          // not among the candidates
     float y[O];
@@ -244,7 +244,7 @@ bool mlp_predict_plan(size_t M, size_t K, size_t N, int precision, maxmulsk_plan
     maxmulsk_plan cands[O];
     const int n = candidate_plans(cls, cands, O);
     const size_t max_workspace = (64u << 20) + 4 * sizeof(float) * (M * K + K * N + M * N);
-    int best = -1;
+    int best = -1, second = -1;
     for (int i = 0; i < n; i++) {
         if (precision != MAXMULSK_PREC_FP32 && precision != MAXMULSK_PREC_SPLIT_AUTO &&
             cands[i].precision != precision)
@@ -253,10 +253,13 @@ bool mlp_predict_plan(size_t M, size_t K, size_t N, int precision, maxmulsk_plan
         // Plans with outsized split-K scratch were never timed (the autotuner
         // masks them), so the model's estimate for them means nothing.
         if (workspace_bytes(M, K, N, cands[i]) > max_workspace) continue;
-        if (best < 0 || y[i] < y[best]) best = i;
+        if (best < 0 || y[i] < y[best]) { second = best; best = i; }
+        else if (second < 0 || y[i] < y[second]) second = i;
     }
     if (best < 0) return false;
     *out = cands[best];
+    // Predicted log-time gap to the runner-up (infinite with one candidate).
+    if (margin) *margin = second < 0 ? INFINITY : y[second] - y[best];
     return true;
 }
 

@@ -17,7 +17,9 @@ int mlp_load(const char* path);
 void mlp_unload();
 // Host forward pass of the loaded model: predicted log-time per candidate.
 bool mlp_predict_host(size_t M, size_t K, size_t N, int cls, float* y);
-// Picks the candidate with the lowest predicted time, if a model is loaded.
-bool mlp_predict_plan(size_t M, size_t K, size_t N, int precision, maxmulsk_plan* out);
+// Picks the candidate with the lowest predicted time, if a model is loaded;
+// with `margin`, also the predicted log-time gap between it and the
+// runner-up (how sure the model is of its choice).
+bool mlp_predict_plan(size_t M, size_t K, size_t N, int precision, maxmulsk_plan* out, float* margin = nullptr);
 
 }  // namespace mmsk

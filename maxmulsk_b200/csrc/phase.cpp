@@ -31,7 +31,12 @@ std::mutex g_mu;
 std::vector<Record> g_records;           // recorded since the last report
 constexpr size_t kMaxRecords = 1 << 16;  // beyond this, scopes record nothing until the next report
 
+thread_local int t_muted = 0;             // PhaseMute nesting depth on this thread
+
 }  // namespace
+
+PhaseMute::PhaseMute() { t_muted++; }
+PhaseMute::~PhaseMute() { t_muted--; }
 
 bool phase_timing_on() {
     int v = g_on.load(std::memory_order_relaxed);
@@ -46,7 +51,7 @@ bool phase_timing_on() {
 void phase_set(bool on) { g_on.store(on ? 1 : 0); }
 
 PhaseScope::PhaseScope(Phase phase, cudaStream_t stream) : phase_(phase), stream_(stream) {
-    if (!phase_timing_on()) return;
+    if (t_muted > 0 || !phase_timing_on()) return;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
     if (cudaEventCreate(&begin_) != cudaSuccess) { begin_ = nullptr; return; }

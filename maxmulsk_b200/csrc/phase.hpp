@@ -34,6 +34,16 @@ void phase_set(bool on);
 // truncated to len, forgets them, and returns the length of the whole text.
 size_t phase_report(char* buf, size_t len);
 
+// While a PhaseMute lives, scopes on this host thread record nothing (the
+// autotuner's timing runs are not phases of the caller's call).
+class PhaseMute {
+public:
+    PhaseMute();
+    ~PhaseMute();
+    PhaseMute(const PhaseMute&) = delete;
+    PhaseMute& operator=(const PhaseMute&) = delete;
+};
+
 class PhaseScope {
 public:
     PhaseScope(Phase phase, cudaStream_t stream);

@@ -7,11 +7,16 @@
 //   choose_rule     SMEKernels1x4V4C::choose  sme/v4/sme-1x4-v4c-dispatch.cpp:17-22
 //   choose_tuned    MaxMulSK::tuning::select  sme/support/gemm_tuning.cpp:96-100
 //   parse_config_env parse_env(MAXMULSK_BLOCKING)  sme/support/gemm_tuning.cpp:66-78
+//   picker_doubt    when the learned model is not to be trusted and the
+//                   exhaustive search (autotune.cpp) runs instead; the
+//                   reference's counterpart is the MAXMULSK_BLOCKING sweep
+//                   that overrides its table (gemm_tuning.cpp:66-78, 96-100)
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
 #include "internal.hpp"
+#include "mlp.hpp"
 #include "runtime.hpp"
 #include "tuning.hpp"
 
@@ -137,6 +142,41 @@ maxmulsk_plan choose_tuned(size_t M, size_t K, size_t N, int precision, int sms)
     if (tuning_lookup(M, K, N, precision, &p)) return p;
     if (tuning_predict(M, K, N, precision, &p)) return p;
     return choose_rule(M, K, N, precision, sms);
+}
+
+namespace {
+// The learned model was trained on M, N, K in [1, 16384].
+constexpr size_t kTrainedMaxDim = 16384;
+
+double env_double(const char* name, double dflt) {
+    const char* s = std::getenv(name);
+    if (!s || !*s) return dflt;
+    char* end = nullptr;
+    const double v = std::strtod(s, &end);
+    return (end && *end == '\0') ? v : dflt;
+}
+}  // namespace
+
+bool autotune_fallback_enabled() {
+    const char* s = std::getenv("MAXMULSK_AUTOTUNE");
+    return !(s && std::strcmp(s, "0") == 0);
+}
+
+const char* picker_doubt(size_t M, size_t K, size_t N, int precision) {
+    // BF16X9 has no candidates of its own: the autotuner does not search it.
+    if (precision == MAXMULSK_PREC_BF16X9) return nullptr;
+    maxmulsk_plan p;
+    if (tuning_lookup(M, K, N, precision, &p)) return nullptr;
+    float margin = 0.f;
+    if (!mlp_predict_plan(M, K, N, precision, &p, &margin)) return "no learned model";
+    if (M > kTrainedMaxDim || N > kTrainedMaxDim || K > kTrainedMaxDim) return "shape outside the trained range";
+    // Predicted ln-time gap to the runner-up. Measured on the committed
+    // held-out timings, the gap barely predicts the model's regret (FP32:
+    // 1.8 % mean regret below 0.005, 2.3 % above), so the search pays in
+    // proportion to how often it runs; the default 0.005 sends about a sixth
+    // of new shapes to it.
+    if ((double)margin < env_double("MAXMULSK_AUTOTUNE_MARGIN", 0.005)) return "close call";
+    return nullptr;
 }
 
 }  // namespace mmsk

@@ -129,23 +129,7 @@ maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t
     DeviceState* ds = current_state();
     if (!ds->err_word) { set_error_message("device error word unavailable"); return MAXMULSK_ERR_ALLOC; }
 
-    if (plan.precision == MAXMULSK_PREC_FP32) {
-        SimtArgs a{};
-        a.A = dA; a.B = dB; a.C = dC;
-        a.M = (int64_t)M; a.K = (int64_t)K; a.N = (int64_t)N;
-        a.kchunk = (int64_t)slice_len(K, plan.split_k);
-        a.splits = slice_count(K, plan.split_k);
-        if (!simt_bind_workspace(a, plan.tile_m, plan.tile_n, ws, ws_bytes)) {
-            set_error_message("workspace too small for the SIMT plan");
-            return MAXMULSK_ERR_INVALID;
-        }
-        if (a.splits > 1) {
-            const size_t tiles = (size_t)((M + plan.tile_m - 1) / plan.tile_m) * ((N + plan.tile_n - 1) / plan.tile_n);
-            st = cuda_status(cudaMemsetAsync(a.counters, 0, tiles * sizeof(unsigned), s), "cudaMemsetAsync(counters)");
-            if (st != MAXMULSK_OK) return st;
-        }
-        return cuda_status(simt_launch(a, plan.tile_m, plan.tile_n, plan.variant, s), "sgemm_simt launch");
-    }
+    if (plan.precision == MAXMULSK_PREC_FP32) return simt_run(dA, dB, dC, M, K, N, plan, ws, ws_bytes, s);
 
     if (ds->major != 10) {
         set_error_message("split-precision tensor-core kernels need an sm_100 device");
@@ -179,6 +163,33 @@ maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t
     return cuda_status(tc_launch(a, s), "sgemm_split_tc launch");
 }
 
+void* managed_workspace(cudaStream_t s, size_t need, size_t* bytes, maxmulsk_status* st) {
+    *st = MAXMULSK_OK;
+    DeviceState* ds = current_state();
+    std::lock_guard<std::mutex> lk(ds->mu);
+    Workspace& w = ds->ws[s];
+    if (w.bytes < need) {
+        // The old buffer may still be read by work queued on this stream.
+        if (w.ptr) {
+            *st = cuda_status(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+            if (*st != MAXMULSK_OK) return nullptr;
+            cudaFree(w.ptr);
+            w.ptr = nullptr;
+            w.bytes = 0;
+        }
+        size_t grown = need + need / 4;
+        cudaError_t e = cudaMalloc(&w.ptr, grown);
+        if (e != cudaSuccess) {
+            w.ptr = nullptr;
+            *st = cuda_status(e, "cudaMalloc(workspace)");
+            return nullptr;
+        }
+        w.bytes = grown;
+    }
+    *bytes = w.bytes;
+    return w.ptr;
+}
+
 maxmulsk_status run_plan_managed(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
                                  const maxmulsk_plan& plan, cudaStream_t s, void* b_planes) {
     maxmulsk_status st = classify_plan(M, K, N, &plan);
@@ -188,28 +199,8 @@ maxmulsk_status run_plan_managed(const float* dA, const float* dB, float* dC, si
     void* ws = nullptr;
     size_t ws_bytes = 0;
     if (need > 0) {
-        DeviceState* ds = current_state();
-        std::lock_guard<std::mutex> lk(ds->mu);
-        Workspace& w = ds->ws[s];
-        if (w.bytes < need) {
-            // The old buffer may still be read by work queued on this stream.
-            if (w.ptr) {
-                st = cuda_status(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-                if (st != MAXMULSK_OK) return st;
-                cudaFree(w.ptr);
-                w.ptr = nullptr;
-                w.bytes = 0;
-            }
-            size_t grown = need + need / 4;
-            cudaError_t e = cudaMalloc(&w.ptr, grown);
-            if (e != cudaSuccess) {
-                w.ptr = nullptr;
-                return cuda_status(e, "cudaMalloc(workspace)");
-            }
-            w.bytes = grown;
-        }
-        ws = w.ptr;
-        ws_bytes = w.bytes;
+        ws = managed_workspace(s, need, &ws_bytes, &st);
+        if (!ws) return st;
     }
     return run_plan_dev(dA, dB, dC, M, K, N, plan, ws, ws_bytes, s, b_planes);
 }
@@ -336,6 +327,28 @@ maxmulsk_status host_pipelined(HostStage& hs, const float* A, const float* B, fl
 }
 
 }  // namespace
+
+void autotune_fallback_host(const float* A, const float* B, size_t M, size_t K, size_t N, int precision) {
+    if (M == 0 || N == 0 || K == 0 || !A || !B) return;
+    if (!autotune_fallback_enabled() || !picker_doubt(M, K, N, precision)) return;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return;
+    HostStage& hs = t_stage[dev];
+    if (!hs.stream && cudaStreamCreateWithFlags(&hs.stream, cudaStreamNonBlocking) != cudaSuccess) {
+        hs.stream = nullptr;
+        return;
+    }
+    if (grow(&hs.dA, &hs.capA, M * K) != cudaSuccess || grow(&hs.dB, &hs.capB, K * N) != cudaSuccess ||
+        grow(&hs.dC, &hs.capC, M * N) != cudaSuccess)
+        return;
+    cudaStream_t s = hs.stream;
+    if (cudaMemcpyAsync(hs.dA, A, M * K * sizeof(float), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(hs.dB, B, K * N * sizeof(float), cudaMemcpyHostToDevice, s) != cudaSuccess) {
+        cudaStreamSynchronize(s);
+        return;
+    }
+    autotune_fallback(hs.dA, hs.dB, hs.dC, M, K, N, precision, s);
+}
 
 maxmulsk_status run_plan_host(const float* A, const float* B, float* C, size_t M, size_t K, size_t N,
                               const maxmulsk_plan& plan) {

@@ -23,6 +23,25 @@ size_t workspace_bytes(size_t M, size_t K, size_t N, const maxmulsk_plan& plan);
 maxmulsk_plan choose_rule(size_t M, size_t K, size_t N, int precision, int sms);
 maxmulsk_plan choose_tuned(size_t M, size_t K, size_t N, int precision, int sms);
 bool parse_config_env(maxmulsk_plan& out);
+// Exhaustive search as the picker's fallback. picker_doubt says why the
+// learned model should not decide this shape (no model loaded, a shape
+// outside its training range, two plans predicted within
+// MAXMULSK_AUTOTUNE_MARGIN, default 0.005 in ln-time), or nullptr when the
+// model (or a tuning database entry) decides. MAXMULSK_AUTOTUNE=0 turns the
+// fallback off.
+const char* picker_doubt(size_t M, size_t K, size_t N, int precision);
+bool autotune_fallback_enabled();
+// Runs the search on these device operands when it is due (enabled, no
+// database entry, picker_doubt, `s` not being captured into a graph) and
+// stores the winner in the tuning database; C is overwritten by the search.
+// Failures leave the picker to the model or the rule.
+void autotune_fallback(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N, int precision,
+                       cudaStream_t s);
+// Host-pointer form: copies A and B to this thread's device staging first.
+void autotune_fallback_host(const float* A, const float* B, size_t M, size_t K, size_t N, int precision);
+// The library-managed workspace of (current device, stream), grown to at
+// least `need` bytes (it may synchronise `s` to grow); nullptr on failure.
+void* managed_workspace(cudaStream_t s, size_t need, size_t* bytes, maxmulsk_status* st);
 
 // Runs a validated plan on device pointers with a caller-provided workspace.
 // b_planes (split-precision plans only): B's operand planes, already written

@@ -20,9 +20,11 @@
 // Edges (the reference's scratch-tile path, :539-558) are predicated loads
 // that read zero outside the matrix and predicated stores; C outside the
 // matrix is never touched.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <mutex>
+#include <vector>
 
 #include "internal.hpp"
 #include "phase.hpp"
@@ -380,6 +382,27 @@ cudaError_t simt_launch(const SimtArgs& a, int tile_m, int tile_n, int variant, 
     return cudaErrorInvalidValue;
 }
 
+maxmulsk_status simt_run(const float* dA, const float* dB, float* dC, size_t M, size_t K, size_t N,
+                         const maxmulsk_plan& plan, void* scratch, size_t scratch_bytes, cudaStream_t s) {
+    SimtArgs a{};
+    a.A = dA; a.B = dB; a.C = dC;
+    a.M = (int64_t)M; a.K = (int64_t)K; a.N = (int64_t)N;
+    a.kchunk = (int64_t)slice_len(K, plan.split_k);
+    a.splits = slice_count(K, plan.split_k);
+    if (!simt_bind_workspace(a, plan.tile_m, plan.tile_n, scratch, scratch_bytes)) {
+        set_error_message("workspace too small for the SIMT plan");
+        return MAXMULSK_ERR_INVALID;
+    }
+    if (a.splits > 1) {
+        // The split-K arrival counters must start at zero on every call.
+        const size_t tiles = (size_t)((M + plan.tile_m - 1) / plan.tile_m) * ((N + plan.tile_n - 1) / plan.tile_n);
+        maxmulsk_status st =
+            cuda_status(cudaMemsetAsync(a.counters, 0, tiles * sizeof(unsigned), s), "cudaMemsetAsync(counters)");
+        if (st != MAXMULSK_OK) return st;
+    }
+    return cuda_status(simt_launch(a, plan.tile_m, plan.tile_n, plan.variant, s), "sgemm_simt launch");
+}
+
 namespace {
 template <int BM, int BN>
 cudaError_t launch_grouped_tile(const GroupProblem* probs, const GroupUnit* units, int nunits, unsigned* next,
@@ -420,7 +443,9 @@ cudaError_t simt_grouped_launch(const GroupProblem* probs, const GroupUnit* unit
 //     serialised by the caller;
 //   * the first call on a device resolves the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture;
+//     before any stream capture. The address is kept per CUDA context, so a
+//     context made after cudaDeviceReset resolves it again (its first call,
+//     too, belongs before any capture);
 //   * the array keeps the last call's contents; the arrival counters that
 //     must start at zero are cleared on the stream before every launch.
 // ---------------------------------------------------------------------------
@@ -428,25 +453,61 @@ static __device__ __align__(256) unsigned char g_simt_static_scratch[MAXMULSK_ST
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_static_mu;
-void* g_static_addr[kMaxDevices] = {};
+// The array's device address is resolved once per CUDA context (the primary
+// context of each device the library is used on), keyed on the context's
+// process-unique id (cuCtxGetId), so a context created after cudaDeviceReset
+// resolves it again instead of reusing an address that no longer exists.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
 
-// Device address of g_simt_static_scratch on the current device, resolved
-// once per device.
+struct StaticAddr {
+    int device;
+    unsigned long long ctx_id;
+    void* ptr;
+};
+std::mutex g_static_mu;
+std::vector<StaticAddr> g_static_addr;
+
+template <typename Fn>
+Fn driver_fn(const char* name) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+        return reinterpret_cast<Fn>(p);
+    return nullptr;
+}
+
+// Id of the current context (0 when the driver cannot say, which then keys
+// the cache on the device alone).
+unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_ctx = driver_fn<CtxGetCurrentFn>("cuCtxGetCurrent");
+    static CtxGetIdFn get_id = driver_fn<CtxGetIdFn>("cuCtxGetId");
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (get_ctx && get_id && get_ctx(&c) == CUDA_SUCCESS && c && get_id(c, &id) == CUDA_SUCCESS) return id;
+    return 0;
+}
+
+// Device address of g_simt_static_scratch in the current context. A thread
+// with no context bound yet (id 0) resolves the address, which binds the
+// device's primary context, and records it under that context's id.
 cudaError_t static_scratch_address(void** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    unsigned long long ctx = current_context_id();
     std::lock_guard<std::mutex> lk(g_static_mu);
-    if (!g_static_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_simt_static_scratch);
-        if (e != cudaSuccess) return e;
-        g_static_addr[dev] = p;
-    }
-    *out = g_static_addr[dev];
+    if (ctx != 0)
+        for (const StaticAddr& a : g_static_addr)
+            if (a.device == dev && a.ctx_id == ctx) { *out = a.ptr; return cudaSuccess; }
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_simt_static_scratch);
+    if (e != cudaSuccess) return e;
+    ctx = current_context_id();
+    for (StaticAddr& a : g_static_addr)
+        if (a.device == dev) { a.ctx_id = ctx; a.ptr = p; *out = p; return cudaSuccess; }
+    g_static_addr.push_back(StaticAddr{dev, ctx, p});
+    *out = p;
     return cudaSuccess;
 }
 
@@ -467,24 +528,12 @@ maxmulsk_status simt_run_static_scratch(const float* dA, const float* dB, float*
         set_error_message("plan needs more scratch than the static maximum of MAXMULSK_STATIC_SCRATCH_BYTES (16 MiB)");
         return MAXMULSK_ERR_UNSUPPORTED;
     }
-    SimtArgs a{};
-    a.A = dA; a.B = dB; a.C = dC;
-    a.M = (int64_t)M; a.K = (int64_t)K; a.N = (int64_t)N;
-    a.kchunk = (int64_t)slice_len(K, plan.split_k);
-    a.splits = slice_count(K, plan.split_k);
+    void* base = nullptr;
     if (need > 0) {
-        void* base = nullptr;
         st = cuda_status(static_scratch_address(&base), "cudaGetSymbolAddress(static scratch)");
         if (st != MAXMULSK_OK) return st;
-        if (!simt_bind_workspace(a, plan.tile_m, plan.tile_n, base, need)) {
-            set_error_message("static scratch binding failed");
-            return MAXMULSK_ERR_INVALID;
-        }
-        const size_t tiles = (size_t)((M + plan.tile_m - 1) / plan.tile_m) * ((N + plan.tile_n - 1) / plan.tile_n);
-        st = cuda_status(cudaMemsetAsync(a.counters, 0, tiles * sizeof(unsigned), s), "cudaMemsetAsync(counters)");
-        if (st != MAXMULSK_OK) return st;
     }
-    return cuda_status(simt_launch(a, plan.tile_m, plan.tile_n, plan.variant, s), "sgemm_simt launch (static scratch)");
+    return simt_run(dA, dB, dC, M, K, N, plan, base, need, s);
 }
 
 }  // namespace mmsk

@@ -7,7 +7,7 @@ Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
   restatement: FP32 scalar GEMM (Utils::multiply_scalar), the v3 outer-Kc
   panel order, FP64 truth, error measures, split planes, seeded generators.
 * ``libmaxmulsk_ref.so`` (oracle/_ref/, built from the reference checkout's
-  common/utils.hpp by ``make -C oracle ref``): the reference's own
+  common/utils.hpp by ``make -C oracle ref REFERENCE_ROOT=<checkout>``): the reference's own
   multiply_scalar / check_correctness, used to pin the restatement and as the
   timed CPU baseline. Present only where it was built.
 """
@@ -24,25 +24,25 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libmaxmulsk_ref.so")
 REF_FMA_LIB = os.path.join(HERE, "_ref", "libmaxmulsk_ref_fma.so")
-REFERENCE_ROOT = os.environ.get("MAXMULSK_REFERENCE_ROOT", "/root/reference")
 
 _lib = None
 _ref = None
 _ref_fma = None
 
 
-def build(ref: bool = True) -> None:
-    """Compiles the oracle (and the reference wrapper when its sources exist)."""
+def build(reference_root: str | None = None) -> None:
+    """Compiles the oracle, and the reference's own common/utils.hpp into
+    oracle/_ref when `reference_root` names a reference checkout that has it."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if ref and os.path.exists(os.path.join(REFERENCE_ROOT, "common", "utils.hpp")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE_ROOT={REFERENCE_ROOT}"], check=True)
+    if reference_root and os.path.exists(os.path.join(reference_root, "common", "utils.hpp")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE_ROOT={reference_root}"], check=True)
 
 
 def lib() -> ctypes.CDLL:
     global _lib
     if _lib is None:
         if not os.path.exists(LIB):
-            build(ref=False)
+            build()
         L = ctypes.CDLL(LIB)
         fp = POINTER(c_float)
         dp = POINTER(c_double)
@@ -52,6 +52,7 @@ def lib() -> ctypes.CDLL:
         L.oracle_sgemm_scalar.argtypes = [fp, fp, fp, c_size_t, c_size_t, c_size_t]
         L.oracle_sgemm_panels.argtypes = [fp, fp, fp, c_size_t, c_size_t, c_size_t, c_size_t, c_int]
         L.oracle_dgemm.argtypes = [fp, fp, dp, c_size_t, c_size_t, c_size_t, c_int]
+        L.oracle_dgemm_abs.argtypes = [fp, fp, dp, c_size_t, c_size_t, c_size_t]
         L.oracle_dgemm_rows.argtypes = [fp, fp, dp, c_size_t, c_size_t, POINTER(c_int64), c_size_t]
         L.oracle_errors.argtypes = [fp, dp, fp, fp, c_size_t, c_size_t, c_size_t, dp]
         L.oracle_relfrob.argtypes = [fp, fp, c_size_t]
@@ -148,6 +149,13 @@ def sgemm_panels(A: np.ndarray, B: np.ndarray, M: int, K: int, N: int, kc: int =
 def dgemm(A: np.ndarray, B: np.ndarray, M: int, K: int, N: int, threads: int | None = None) -> np.ndarray:
     C = np.empty(M * N, np.float64)
     lib().oracle_dgemm(_f(A), _f(B), _d(C), M, K, N, threads or min(8, os.cpu_count() or 1))
+    return C.reshape(M, N)
+
+
+def dgemm_abs(A: np.ndarray, B: np.ndarray, M: int, K: int, N: int) -> np.ndarray:
+    """(|A||B|)_ij in FP64, k upward (the max-relative floor's sums)."""
+    C = np.empty(M * N, np.float64)
+    lib().oracle_dgemm_abs(_f(A), _f(B), _d(C), M, K, N)
     return C.reshape(M, N)
 
 

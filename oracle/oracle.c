@@ -164,6 +164,21 @@ void oracle_dgemm(const float* A, const float* B, double* C,
     for (int t = 0; t < launched; t++) pthread_join(th[t], NULL);
 }
 
+/* (|A||B|)_ij in FP64, one row after another, k upward: the floor of the
+ * max-relative measure below, formed for every element (the GPU check
+ * product's companion output is compared with it bit for bit). */
+void oracle_dgemm_abs(const float* A, const float* B, double* C, size_t M, size_t K, size_t N) {
+    for (size_t i = 0; i < M; i++) {
+        double* dst = C + i * N;
+        for (size_t c = 0; c < N; c++) dst[c] = 0.0;
+        for (size_t k = 0; k < K; k++) {
+            double a = fabs((double)A[i * K + k]);
+            const float* b = B + k * N;
+            for (size_t c = 0; c < N; c++) dst[c] += a * fabs((double)b[c]);
+        }
+    }
+}
+
 /* FP64 value of selected rows only (sampled checks of large products). */
 void oracle_dgemm_rows(const float* A, const float* B, double* C,
                        size_t K, size_t N, const int64_t* rows, size_t nrows) {

@@ -14,8 +14,9 @@ Shapes: the reference's SME correctness cases (sme/support/test_sme.cpp:28-37),
 its NEON tail cases (neon/test_neon.cpp:20-40, fields M, N, K there) and one
 narrow-M shape of its LLM sweep (bench/results/2026-09-13/source/bench_sweep_shapes.h:4).
 
-Run in a container that has the reference checkout:
-    make -C oracle all ref && python tests/golden/make_golden.py
+Run where the reference checkout is, naming it:
+    make -C oracle all ref REFERENCE_ROOT=<checkout>
+    MAXMULSK_REFERENCE_ROOT=<checkout> python tests/golden/make_golden.py
 """
 from __future__ import annotations
 
@@ -52,7 +53,7 @@ def cases():
 
 def main() -> None:
     if not (oracle.ref_available() and oracle.ref_fma_available()):
-        oracle.build(ref=True)
+        oracle.build(reference_root=os.environ.get("MAXMULSK_REFERENCE_ROOT"))
     rng_pick = np.random.default_rng(20261203)
     records = []
     for i, (M, K, N, tag) in enumerate(cases()):

@@ -24,10 +24,16 @@ def test_binding_table_covers_header(built_lib):
     assert set(_lib.exported_symbols()) <= set(_lib._SIGNATURES) | {"maxmulsk_stream_status"}
 
 
-def test_library_is_built_for_sm100a(built_lib):
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", _lib.LIB_PATH],
-                         capture_output=True, text=True).stdout
-    assert "sm_100a" in out
+def test_library_is_built_for_sm100a_only(built_lib):
+    # Every CUDA source is compiled with exactly one target, sm_100a (no PTX
+    # for other architectures, no multi-arch fat binary): the flags build.py
+    # passes to nvcc for .cu sources, host sources and the link.
+    from maxmulsk_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    for flags in (build.CUFLAGS, build.CXXFLAGS, build.LINKFLAGS):
+        gencodes = [flags[i + 1] for i, f in enumerate(flags) if f == "-gencode"]
+        assert gencodes == ["arch=compute_100a,code=sm_100a"], flags
+        assert not any(f.startswith(("-arch", "--gpu-architecture")) for f in flags), flags
 
 
 def test_status_codes_keep_reference_values(built_lib):

@@ -109,9 +109,7 @@ def test_grouped_benchmark_batch_sampled(cuda, oracle_mod):
     rng = np.random.default_rng(0)
     for i in rng.choice(len(shapes), 12, replace=False):
         M, K, N = shapes[i]
-        ref = As[i].view(M, K).double() @ Bs[i].view(K, N).double()
-        err = float(torch.linalg.norm(Cs[i].view(M, N).double() - ref) /
-                    (torch.linalg.norm(As[i].double()) * torch.linalg.norm(Bs[i].double())))
+        err = mm.Fp64Check(As[i], Bs[i], M, K, N, with_abs=False).errors(Cs[i])["normwise"]
         assert err < 4 * 2.0 ** -24 * np.sqrt(K), (shapes[i], err)
     for c in Cs:
         assert not bool(torch.isnan(c).any())
@@ -186,9 +184,7 @@ def test_grouped_benchmark_batch_split_precision(cuda):
     rng = np.random.default_rng(1)
     for i in rng.choice(len(shapes), 16, replace=False):
         M, K, N = shapes[i]
-        ref = As[i].view(M, K).double() @ Bs[i].view(K, N).double()
-        err = float(torch.linalg.norm(Cs[i].view(M, N).double() - ref) /
-                    (torch.linalg.norm(As[i].double()) * torch.linalg.norm(Bs[i].double())))
+        err = mm.Fp64Check(As[i], Bs[i], M, K, N, with_abs=False).errors(Cs[i])["normwise"]
         assert err < 4 * 2.0 ** -24 * np.sqrt(K), (shapes[i], err)
     for c in Cs:
         assert not bool(torch.isnan(c).any())

@@ -110,3 +110,168 @@ def test_trained_picker_regret_on_held_out_shapes(cuda):
     assert r_mlp["rows"] == r_rule["rows"] == 1000
     assert r_mlp["mean"] <= 0.05 and r_mlp["geomean"] <= 0.05 and r_mlp["total_time"] <= 0.05, r_mlp
     assert r_mlp["total_time"] < r_rule["total_time"] and r_mlp["geomean"] < r_rule["geomean"], (r_mlp, r_rule)
+
+
+# --------------------------------------------------------------------------- exhaustive search as the fallback
+def _shipped_model():
+    import os
+    return os.path.join(os.path.dirname(picker.__file__), "data", "picker_model.bin").encode()
+
+
+def _db_entries(tmp_path) -> int:
+    path = str(tmp_path / "db_count.txt")
+    return int(mm.lib().maxmulsk_tuning_save(path.encode()))
+
+
+def _rand(torch, n):
+    return torch.rand(n, device="cuda") * 2 - 1
+
+
+@pytest.fixture
+def clean_picker(monkeypatch):
+    for v in ("MAXMULSK_AUTOTUNE", "MAXMULSK_AUTOTUNE_MARGIN", "MAXMULSK_CONFIG"):
+        monkeypatch.delenv(v, raising=False)
+    mm.lib().maxmulsk_tuning_clear()
+    yield
+    mm.lib().maxmulsk_tuning_clear()
+    assert mm.lib().maxmulsk_model_load(_shipped_model()) == 0
+
+
+def test_fallback_searches_without_a_model(cuda, clean_picker, tmp_path):
+    # No learned model: the device entry searches the candidates on its own
+    # operands, stores the winner, and runs it; the query then returns it.
+    torch = cuda
+    M, K, N = 300, 1500, 260
+    mm.lib().maxmulsk_model_load(None)
+    assert mm.picker_doubt(M, K, N) == "no learned model"
+    rule = mm.choose(M, K, N).as_tuple()
+    assert rule == mm.choose_rule(M, K, N).as_tuple()
+    dA, dB, dC = _rand(torch, M * K), _rand(torch, K * N), torch.empty(M * N, device="cuda")
+    assert mm.sgemm_v3_dev(dA, dB, dC, M, K, N) == 0 and mm.stream_status() == 0
+    assert _db_entries(tmp_path) == 1
+    assert mm.picker_doubt(M, K, N) is None                  # the database decides from now on
+    tuned = mm.choose(M, K, N)
+    # the call ran the stored plan: same bits as that plan run explicitly
+    dC2 = torch.empty(M * N, device="cuda")
+    nb = mm.workspace_bytes(M, K, N, tuned)
+    ws = torch.empty(nb + 256, dtype=torch.uint8, device="cuda")
+    assert mm.sgemm_plan_dev(dA, dB, dC2, M, K, N, tuned, ws.data_ptr() + ((-ws.data_ptr()) % 256), nb) == 0
+    assert bool(torch.equal(dC, dC2))
+    # split precision takes the same route (its own database key)
+    assert mm.sgemm_split_dev(dA, dB, dC, M, K, N, mm.Precision.SPLIT_AUTO) == 0 and mm.stream_status() == 0
+    assert _db_entries(tmp_path) == 2
+
+
+def test_fallback_searches_outside_the_trained_range(cuda, clean_picker, tmp_path):
+    torch = cuda
+    M, K, N = 48, 20000, 40
+    assert mm.picker_doubt(M, K, N) == "shape outside the trained range"
+    dA, dB, dC = _rand(torch, M * K), _rand(torch, K * N), torch.empty(M * N, device="cuda")
+    assert mm.sgemm_v3_dev(dA, dB, dC, M, K, N) == 0 and mm.stream_status() == 0
+    assert _db_entries(tmp_path) == 1
+
+
+def test_fallback_on_close_calls_and_its_switch(cuda, clean_picker, monkeypatch, tmp_path):
+    torch = cuda
+    M, K, N = 200, 700, 180
+    dA, dB, dC = _rand(torch, M * K), _rand(torch, K * N), torch.empty(M * N, device="cuda")
+    monkeypatch.setenv("MAXMULSK_AUTOTUNE_MARGIN", "0")          # the model decides
+    assert mm.sgemm_v3_dev(dA, dB, dC, M, K, N) == 0 and mm.stream_status() == 0
+    assert _db_entries(tmp_path) == 0
+    monkeypatch.setenv("MAXMULSK_AUTOTUNE_MARGIN", "100")        # every shape is a close call
+    monkeypatch.setenv("MAXMULSK_AUTOTUNE", "0")                 # ... but the fallback is off
+    assert mm.sgemm_v3_dev(dA, dB, dC, M, K, N) == 0 and mm.stream_status() == 0
+    assert _db_entries(tmp_path) == 0
+    monkeypatch.delenv("MAXMULSK_AUTOTUNE")
+    C_host = np.empty(M * N, np.float32)                          # the host entry searches too
+    assert mm.sgemm_v3(dA.cpu().numpy(), dB.cpu().numpy(), C_host, M, K, N) == 0, mm.last_error_message()
+    assert _db_entries(tmp_path) == 1
+
+
+def test_fallback_never_runs_inside_a_stream_capture(cuda, clean_picker, monkeypatch, tmp_path):
+    # A caller capturing its stream into a CUDA graph gets the model's (here,
+    # with no model, the rule's) plan captured; nothing is timed or
+    # synchronised during the capture, and the database stays empty.
+    torch = cuda
+    M, K, N = 160, 900, 96
+    mm.lib().maxmulsk_model_load(None)
+    dA, dB, dC = _rand(torch, M * K), _rand(torch, K * N), torch.empty(M * N, device="cuda")
+    s = torch.cuda.Stream()
+    # first call outside the capture with the search off: sizes the stream's workspace
+    monkeypatch.setenv("MAXMULSK_AUTOTUNE", "0")
+    assert mm.sgemm_v3_dev(dA, dB, dC, M, K, N, s) == 0
+    torch.cuda.synchronize()
+    want = dC.clone()
+    monkeypatch.delenv("MAXMULSK_AUTOTUNE")
+    assert mm.picker_doubt(M, K, N) == "no learned model"
+    dC.zero_()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s):
+        st = mm.sgemm_v3_dev(dA, dB, dC, M, K, N, s)
+    assert st == 0
+    assert _db_entries(tmp_path) == 0
+    g.replay()
+    torch.cuda.synchronize()
+    assert bool(torch.equal(dC, want))
+    del g
+
+
+def test_config_env_reaches_the_kernel(cuda, oracle_mod, clean_picker, monkeypatch):
+    # MAXMULSK_CONFIG (the counterpart of MAXMULSK_BLOCKING,
+    # sme/support/gemm_tuning.cpp:66-78) decides what maxmulsk_sgemm_v3 runs:
+    # a 3-slice FP32 plan gives the oracle's 3-panel sum bit for bit; a
+    # malformed value is ignored.
+    M, K, N = 150, 1000, 90
+    A = oracle_mod.fill_uniform(M * K, 5)
+    B = oracle_mod.fill_uniform(K * N, 6)
+    monkeypatch.setenv("MAXMULSK_CONFIG", "0,64,64,3")
+    C = np.empty(M * N, np.float32)
+    assert mm.sgemm_v3(A, B, C, M, K, N) == 0
+    want = oracle_mod.sgemm_panels(A, B, M, K, N, kc=mm.slice_len(K, 3), fma=True)
+    assert np.array_equal(C.view(np.uint32), want.ravel().view(np.uint32))
+    monkeypatch.setenv("MAXMULSK_CONFIG", "0,64,64")
+    monkeypatch.setenv("MAXMULSK_AUTOTUNE", "0")
+    plan = mm.choose(M, K, N)
+    C2 = np.empty(M * N, np.float32)
+    assert mm.sgemm_v3(A, B, C2, M, K, N) == 0
+    want2 = oracle_mod.sgemm_panels(A, B, M, K, N, kc=mm.slice_len(K, plan.split_k), fma=True)
+    assert np.array_equal(C2.view(np.uint32), want2.ravel().view(np.uint32))
+
+
+def test_live_regret_on_fresh_shapes(cuda, clean_picker):
+    # The learned picker against exhaustive search, both timed now on this
+    # GPU (the regret test above scores the committed timing table): 20 fresh
+    # shapes, M, N, K log-uniform in [1, 16384] (product capped so the search
+    # stays short), FP32 and split precision.
+    from maxmulsk_b200 import workloads
+    torch = cuda
+    shapes = [s for s in workloads.picker_shapes(400, seed=9091) if s[0] * s[1] * s[2] <= 2 ** 35][:20]
+    ws_bytes = 1 << 30
+    ws = torch.empty(ws_bytes + 256, dtype=torch.uint8, device="cuda")
+    wp = ws.data_ptr() + ((-ws.data_ptr()) % 256)
+    regrets = {0: [], 1: []}
+    totals = {0: [0.0, 0.0], 1: [0.0, 0.0]}
+    for (M, K, N) in shapes:
+        dA, dB, dC = _rand(torch, M * K), _rand(torch, K * N), torch.empty(M * N, device="cuda")
+        for cls, prec in ((0, mm.Precision.FP32), (1, mm.Precision.SPLIT_AUTO)):
+            cands = autotune.candidates(cls)
+            t = autotune.time_plans(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M, K, N, cands, wp, ws_bytes)
+            pick = mm.choose(M, K, N, prec).as_tuple()
+            idx = [i for i, c in enumerate(cands) if c.as_tuple() == pick]
+            if idx and np.isfinite(t[idx[0]]):
+                t_pick = float(t[idx[0]])
+            else:   # the rule's plan, outside the candidate list: time it alone
+                t_pick = float(autotune.time_plans(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), M, K, N,
+                                                   [mm.choose(M, K, N, prec)], wp, ws_bytes)[0])
+            best = float(np.min(t[np.isfinite(t)]))
+            regrets[cls].append(t_pick / best - 1.0)
+            totals[cls][0] += t_pick
+            totals[cls][1] += best
+    for cls in (0, 1):
+        r = np.array(regrets[cls])
+        total = totals[cls][0] / totals[cls][1] - 1.0
+        print(f"class {cls}: {len(r)} shapes, mean regret {r.mean():.3f}, median {np.median(r):.3f}, "
+              f"total-time {total:.3f}")
+        # single live timings carry a few per cent of noise on both sides
+        assert total <= 0.10 and r.mean() <= 0.10, (cls, r, total)

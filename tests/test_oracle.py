@@ -177,3 +177,68 @@ def test_split_exact_products(oracle_mod):
         C = oracle_mod.sgemm_split_exact(A, B, M, K, N, mode)
         e = oracle_mod.errors(C, C64, A, B, M, K, N)
         assert e["normwise"] < tol, (mode, e)
+
+
+# --------------------------------------------------------------------------- pinning inputs
+def _kept_pairs(mode):
+    if mode == 1:
+        return [(0, 0), (0, 1), (1, 0)]
+    if mode == 2:
+        return [(i, j) for i in range(3) for j in range(3) if i + j <= 2]
+    return [(i, j) for i in range(3) for j in range(3)]
+
+
+@pytest.mark.parametrize("mode,side,level", [(1, "a", 1), (1, "b", 1), (2, "a", 1), (2, "a", 2), (2, "b", 2),
+                                             (3, "a", 1), (3, "b", 2)])
+def test_pinning_inputs_are_exact_in_fp32(oracle_mod, mode, side, level):
+    # The GPU pins compare the tensor-core result with the exact split product
+    # bit for bit; that is sound only if, in the order the hardware may add
+    # them, every partial sum is exact in FP32. One MMA covers one limb pair
+    # over an aligned block of k's, so the two halves of a k pair (whose
+    # leading-limb products cancel) meet inside one MMA. Here: each k pair of
+    # each kept limb pair summed first (exactly), then those sums added in FP32
+    # in k order, in reverse, and limb pair by limb pair -- all equal the
+    # FP64-accumulated exact split product.
+    from pinning import pinning_inputs
+    rng = np.random.default_rng(mode * 100 + level)
+    M, K, N = 9, 64, 11
+    A, B = pinning_inputs(rng, M, K, N, mode, side, level)
+    want = oracle_mod.sgemm_split_exact(A, B, M, K, N, mode)
+    if mode == 1:
+        la, lb = oracle_mod.split_tf32(A), oracle_mod.split_tf32(B)
+    else:
+        la, lb = oracle_mod.split_bf16(A), oracle_mod.split_bf16(B)
+    la = [x.reshape(M, K) for x in la]
+    lb = [x.reshape(K, N) for x in lb]
+    terms = np.stack([la[i][:, :, None] * lb[j][None, :, :] for (i, j) in _kept_pairs(mode)])  # (P, M, K, N)
+    assert terms.dtype == np.float32
+    pairs = terms[:, :, 0::2, :] + terms[:, :, 1::2, :]
+    assert np.array_equal(pairs.astype(np.float64),
+                          terms[:, :, 0::2, :].astype(np.float64) + terms[:, :, 1::2, :].astype(np.float64))
+    P, H = pairs.shape[0], pairs.shape[2]
+    orders = [[(p, h) for h in range(H) for p in range(P)],
+              [(p, h) for p in reversed(range(P)) for h in reversed(range(H))],
+              [(p, h) for p in range(P) for h in range(H)]]
+    for order in orders:
+        acc = np.zeros((M, N), np.float32)
+        for p, h in order:
+            acc = acc + pairs[p, :, h, :]
+        assert np.array_equal(acc, want)
+
+
+def test_pinning_inputs_separate_the_modes(oracle_mod):
+    # On the pinning inputs the modes' exact products differ from one another
+    # and from the full product, so a kernel that computed a different set of
+    # limb products cannot match the pins.
+    from pinning import pinning_inputs
+    rng = np.random.default_rng(7)
+    M, K, N = 16, 32, 24
+    for side in ("a", "b"):
+        for level in (1, 2):
+            A, B = pinning_inputs(rng, M, K, N, 2, side, level)
+            assert not np.array_equal(oracle_mod.sgemm_split_exact(A, B, M, K, N, 2),
+                                      oracle_mod.sgemm_split_exact(A, B, M, K, N, 3)), (side, level)
+        A, B = pinning_inputs(rng, M, K, N, 1, side, 1)
+        tf = oracle_mod.sgemm_split_exact(A, B, M, K, N, 1)
+        full = oracle_mod.dgemm(A, B, M, K, N).astype(np.float32)
+        assert not np.array_equal(tf, full), side

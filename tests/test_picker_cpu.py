@@ -5,6 +5,7 @@ import ctypes
 import math
 
 import numpy as np
+import pytest
 
 import maxmulsk_b200 as mm
 from maxmulsk_b200 import picker
@@ -100,3 +101,90 @@ def test_default_model_beside_the_library(built_lib, tmp_path):
     path = str(tmp_path / "zero.bin")
     picker.save_params(path, p)
     assert _predict_in_fresh_process(path) == 0
+
+
+# --------------------------------------------------------------------------- MAXMULSK_CONFIG
+# The counterpart of the reference's MAXMULSK_BLOCKING override
+# (sme/support/gemm_tuning.cpp:66-78): a well-formed value wins over the
+# picker, a malformed one is ignored.
+SHAPE = (1000, 3000, 700)
+
+
+def test_config_env_overrides_the_picker(built_lib, monkeypatch):
+    M, K, N = SHAPE
+    monkeypatch.delenv("MAXMULSK_CONFIG", raising=False)
+    base_split = mm.choose(M, K, N, mm.Precision.BF16X6).as_tuple()
+    monkeypatch.setenv("MAXMULSK_CONFIG", "2,256,256,4")
+    assert mm.choose(M, K, N, mm.Precision.BF16X6).as_tuple() == (2, 256, 256, 4, 0)
+    monkeypatch.setenv("MAXMULSK_CONFIG", "2,128,128,8,2")
+    assert mm.choose(M, K, N, mm.Precision.BF16X6).as_tuple() == (2, 128, 128, 8, 2)
+    # a configured plan of another precision leaves this precision's pick alone
+    monkeypatch.setenv("MAXMULSK_CONFIG", "0,64,64,4")
+    assert mm.choose(M, K, N, mm.Precision.BF16X6).as_tuple() == base_split
+    assert mm.choose(M, K, N, mm.Precision.FP32).as_tuple() == (0, 64, 64, 4, 0)
+
+
+@pytest.mark.parametrize("bad", ["", "2", "2,128,256", "a,b,c,d", "2,128,256,0", "2,0,256,4", "2,128,-1,4",
+                                 ",,,", "2;128;256;4"])
+def test_malformed_config_env_is_ignored(built_lib, monkeypatch, bad):
+    M, K, N = SHAPE
+    monkeypatch.delenv("MAXMULSK_CONFIG", raising=False)
+    base = {p: mm.choose(M, K, N, p).as_tuple() for p in (mm.Precision.FP32, mm.Precision.BF16X6)}
+    monkeypatch.setenv("MAXMULSK_CONFIG", bad)
+    for p, want in base.items():
+        assert mm.choose(M, K, N, p).as_tuple() == want, (bad, p)
+
+
+# --------------------------------------------------------------------------- exhaustive fallback triggers
+def _load_shipped_model():
+    import os
+    shipped = os.path.join(os.path.dirname(picker.__file__), "data", "picker_model.bin")
+    assert mm.lib().maxmulsk_model_load(shipped.encode()) == 0
+
+
+def test_picker_doubt_triggers(built_lib, monkeypatch):
+    _load_shipped_model()
+    # When the learned model is loaded and the shape is inside its training
+    # range, only a close call sends the picker to exhaustive search; a shape
+    # outside the range always does; MAXMULSK_AUTOTUNE=0 turns it all off.
+    monkeypatch.delenv("MAXMULSK_AUTOTUNE", raising=False)
+    monkeypatch.delenv("MAXMULSK_AUTOTUNE_MARGIN", raising=False)
+    mm.lib().maxmulsk_tuning_clear()
+    assert mm.picker_doubt(100, 20000, 30) == "shape outside the trained range"
+    assert mm.picker_doubt(40000, 64, 64, mm.Precision.BF16X6) == "shape outside the trained range"
+    monkeypatch.setenv("MAXMULSK_AUTOTUNE_MARGIN", "100")
+    assert mm.picker_doubt(512, 512, 512) == "close call"
+    monkeypatch.setenv("MAXMULSK_AUTOTUNE_MARGIN", "0")
+    assert mm.picker_doubt(512, 512, 512) is None
+    assert mm.picker_doubt(512, 512, 512, mm.Precision.BF16X9) is None      # BF16X9 is not searched
+    monkeypatch.setenv("MAXMULSK_AUTOTUNE", "0")
+    assert mm.picker_doubt(100, 20000, 30) is None
+
+
+def test_picker_doubt_without_a_model(built_lib, monkeypatch):
+    monkeypatch.delenv("MAXMULSK_AUTOTUNE", raising=False)
+    mm.lib().maxmulsk_model_load(None)
+    try:
+        assert mm.picker_doubt(512, 512, 512) == "no learned model"
+        assert mm.picker_doubt(512, 512, 512, mm.Precision.SPLIT_AUTO) == "no learned model"
+    finally:
+        _load_shipped_model()
+
+
+def test_close_calls_on_held_out_shapes(built_lib, monkeypatch):
+    # How often the default margin sends a held-out shape to the search, and
+    # what the search saves there: on the committed autotuner timings, the
+    # model's regret on the close calls vs. the rest (the search's own regret
+    # is zero by definition).
+    import os
+    monkeypatch.delenv("MAXMULSK_AUTOTUNE_MARGIN", raising=False)
+    _load_shipped_model()
+    d = dict(np.load(os.path.join(os.path.dirname(picker.__file__), "data", "picker_timings.npz")))
+    ntr = int(d["n_train"])
+    shapes = d["shapes"][ntr:]
+    close = 0
+    for (M, K, N) in shapes[:200]:
+        if mm.picker_doubt(int(M), int(K), int(N)) == "close call":
+            close += 1
+    print("close calls in 200 held-out FP32 shapes:", close)
+    assert 0 <= close <= 200

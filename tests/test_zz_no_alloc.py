@@ -59,6 +59,40 @@ def test_static_scratch_matches_workspace_entry_on_two_calls(cuda, oracle_mod):
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"call {call}"
 
 
+def _static_with_bands(torch, dA, dB, M, K, N, plan, guard=64):
+    """The static entry with C between guard bands of the sentinel (3.75, the
+    reference checker's marker, check_nb.cpp:54); returns (status, C, bands intact)."""
+    buf = torch.full((M * N + 2 * guard,), 3.75, dtype=torch.float32, device="cuda")
+    st = mm.lib().maxmulsk_sgemm_plan_static_dev(dA.data_ptr(), dB.data_ptr(), buf.data_ptr() + 4 * guard, M, K, N,
+                                                 ctypes.byref(plan), None)
+    st2 = mm.stream_status()
+    host = buf.cpu().numpy()
+    C = host[guard: guard + M * N].copy()
+    bands = bool(np.all(host[:guard] == 3.75) and np.all(host[guard + M * N:] == 3.75))
+    return (st if st != 0 else st2), C, bands
+
+
+@pytest.mark.parametrize("plan_args", [(64, 64, 7), (128, 64, 3), (128, 128, 1), (64, 64, 1)])
+def test_static_scratch_edges_and_no_split(cuda, oracle_mod, plan_args):
+    # An odd shape (scalar loads and stores: K and N not multiples of 4,
+    # partial tiles in M and N) with and without a K split, twice with new
+    # inputs: the same bits as the workspace entry, nothing written outside C.
+    from gpu_util import run_plan
+    torch = cuda
+    M, K, N = 97, 1000, 83
+    plan = mm.make_plan(mm.Precision.FP32, *plan_args)
+    assert mm.workspace_bytes(M, K, N, plan) <= STATIC_BYTES
+    for seeds in ((21, 22), (23, 24)):
+        A = oracle_mod.fill_uniform(M * K, seeds[0])
+        B = oracle_mod.fill_wide(K * N, seeds[1])
+        dA, dB = torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda()
+        st, got, bands = _static_with_bands(torch, dA, dB, M, K, N, plan)
+        assert st == 0 and bands, mm.last_error_message()
+        st2, want, bands2 = run_plan(torch, A, B, M, K, N, plan, dA=dA, dB=dB)
+        assert st2 == 0 and bands2
+        assert np.array_equal(got.view(np.uint32), want.ravel().view(np.uint32)), (plan_args, seeds)
+
+
 def test_static_scratch_rejects_plans_beyond_its_size(cuda, oracle_mod):
     torch = cuda
     M, K, N = 512, 8192, 1024
