@@ -22,6 +22,7 @@
 // matrix is never touched.
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 #include <vector>
@@ -56,6 +57,103 @@ struct SimtSmem {
     float Bs[2][kBK][BN];
     int last;
 };
+
+// The end of one tile: without a K split the sums go to C; with one, this
+// slice's partial tile is written and, unless a separate reduction kernel
+// follows, the last CTA of the tile to arrive sums all slices in slice order
+// (C = ((p0 + p1) + p2) + ...). acc[i][4 g + j] is the output at row
+// out_row(i), column out_col(g) + j. `last_flag` is a shared-memory word.
+template <int TM, int GN, class RowFn, class ColFn>
+__device__ __forceinline__ void simt_epilogue(const SimtArgs& p, float (&acc)[TM][4 * GN], RowFn out_row,
+                                              ColFn out_col, bool VEC, int z, unsigned tile, int& last_flag) {
+    const int64_t M = p.M, N = p.N;
+    const int tid = threadIdx.x;
+    if (p.splits <= 1) {
+#pragma unroll
+        for (int i = 0; i < TM; i++) {
+            const int64_t r = out_row(i);
+            if (r >= M) continue;
+#pragma unroll
+            for (int g = 0; g < GN; g++) {
+                const int64_t c = out_col(g);
+                float* dst = p.C + r * N + c;
+                if (VEC && c + 3 < N) {
+                    *reinterpret_cast<float4*>(dst) =
+                        make_float4(acc[i][g * 4 + 0], acc[i][g * 4 + 1], acc[i][g * 4 + 2], acc[i][g * 4 + 3]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; j++)
+                        if (c + j < N) dst[j] = acc[i][g * 4 + j];
+                }
+            }
+        }
+        return;
+    }
+
+    // Split-K: write this slice's partial tile, then the last CTA of the tile
+    // to arrive sums all slices in slice order.
+    const size_t MN = (size_t)M * (size_t)N;
+    float* mine = p.partial + (size_t)z * MN;
+#pragma unroll
+    for (int i = 0; i < TM; i++) {
+        const int64_t r = out_row(i);
+        if (r >= M) continue;
+#pragma unroll
+        for (int g = 0; g < GN; g++) {
+            const int64_t c = out_col(g);
+            if (VEC && c + 3 < N) {
+                __stcg(reinterpret_cast<float4*>(mine + r * N + c),
+                       make_float4(acc[i][g * 4 + 0], acc[i][g * 4 + 1], acc[i][g * 4 + 2], acc[i][g * 4 + 3]));
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    if (c + j < N) __stcg(mine + r * N + c + j, acc[i][g * 4 + j]);
+            }
+        }
+    }
+    if (p.reduce_after) return;                      // summed by simt_splitk_reduce_kernel
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+        unsigned prev = atomicAdd(&p.counters[tile], 1u);
+        last_flag = (prev == (unsigned)(p.splits - 1));
+    }
+    __syncthreads();
+    const int last = last_flag;
+    __syncthreads();                                 // the flag may be rewritten by the next tile
+    if (!last) return;
+    __threadfence();
+    // Each output: slice 0, then every later slice added in slice order; four
+    // adjacent columns at a time with 128-bit loads where rows allow.
+#pragma unroll
+    for (int i = 0; i < TM; i++) {
+        const int64_t r = out_row(i);
+        if (r >= M) continue;
+#pragma unroll
+        for (int g = 0; g < GN; g++) {
+            const int64_t c = out_col(g);
+            const size_t off = (size_t)r * N + c;
+            if (VEC && c + 3 < N) {
+                float4 s4 = __ldcg(reinterpret_cast<const float4*>(p.partial + off));
+                for (int q = 1; q < p.splits; q++) {
+                    const float4 t = __ldcg(reinterpret_cast<const float4*>(p.partial + (size_t)q * MN + off));
+                    s4.x = __fadd_rn(s4.x, t.x); s4.y = __fadd_rn(s4.y, t.y);
+                    s4.z = __fadd_rn(s4.z, t.z); s4.w = __fadd_rn(s4.w, t.w);
+                }
+                *reinterpret_cast<float4*>(p.C + off) = s4;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    if (c + j >= N) continue;
+                    float v = __ldcg(p.partial + off + j);
+                    for (int q = 1; q < p.splits; q++) v = __fadd_rn(v, __ldcg(p.partial + (size_t)q * MN + off + j));
+                    p.C[off + j] = v;
+                }
+            }
+        }
+    }
+    if (tid == 0) p.counters[tile] = 0u;   // leave the counter ready for the next call
+}
 
 // One CTA computes the BM x BN tile at (m0, n0) of K slice z; `tile` numbers
 // the tile for the split-K arrival counters. VM selects 128-bit loads and
@@ -195,87 +293,7 @@ __device__ __forceinline__ void simt_tile(const SimtArgs& p, int64_t m0, int64_t
 
     auto out_row = [&](int i) { return m0 + (i / 4) * 64 + ty * 4 + (i % 4); };
     auto out_col = [&](int g) { return n0 + g * 64 + tx * 4; };
-
-    if (p.splits <= 1) {
-#pragma unroll
-        for (int i = 0; i < TM; i++) {
-            const int64_t r = out_row(i);
-            if (r >= M) continue;
-#pragma unroll
-            for (int g = 0; g < GN; g++) {
-                const int64_t c = out_col(g);
-                float* dst = p.C + r * N + c;
-                if (VEC && c + 3 < N) {
-                    *reinterpret_cast<float4*>(dst) =
-                        make_float4(acc[i][g * 4 + 0], acc[i][g * 4 + 1], acc[i][g * 4 + 2], acc[i][g * 4 + 3]);
-                } else {
-#pragma unroll
-                    for (int j = 0; j < 4; j++)
-                        if (c + j < N) dst[j] = acc[i][g * 4 + j];
-                }
-            }
-        }
-        return;
-    }
-
-    // Split-K: write this slice's partial tile, then the last CTA of the tile
-    // to arrive sums all slices in slice order.
-    const size_t MN = (size_t)M * (size_t)N;
-    float* mine = p.partial + (size_t)z * MN;
-#pragma unroll
-    for (int i = 0; i < TM; i++) {
-        const int64_t r = out_row(i);
-        if (r >= M) continue;
-#pragma unroll
-        for (int g = 0; g < GN; g++) {
-            const int64_t c = out_col(g);
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-                if (c + j < N) __stcg(mine + r * N + c + j, acc[i][g * 4 + j]);
-        }
-    }
-    if (p.reduce_after) return;                      // summed by simt_splitk_reduce_kernel
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) {
-        unsigned prev = atomicAdd(&p.counters[tile], 1u);
-        sm.last = (prev == (unsigned)(p.splits - 1));
-    }
-    __syncthreads();
-    const int last = sm.last;
-    __syncthreads();                                 // sm.last may be rewritten by the next tile
-    if (!last) return;
-    __threadfence();
-    // Each output: slice 0, then every later slice added in slice order; four
-    // adjacent columns at a time with 128-bit loads where rows allow.
-#pragma unroll
-    for (int i = 0; i < TM; i++) {
-        const int64_t r = out_row(i);
-        if (r >= M) continue;
-#pragma unroll
-        for (int g = 0; g < GN; g++) {
-            const int64_t c = out_col(g);
-            const size_t off = (size_t)r * N + c;
-            if (VEC && c + 3 < N) {
-                float4 s4 = __ldcg(reinterpret_cast<const float4*>(p.partial + off));
-                for (int q = 1; q < p.splits; q++) {
-                    const float4 t = __ldcg(reinterpret_cast<const float4*>(p.partial + (size_t)q * MN + off));
-                    s4.x = __fadd_rn(s4.x, t.x); s4.y = __fadd_rn(s4.y, t.y);
-                    s4.z = __fadd_rn(s4.z, t.z); s4.w = __fadd_rn(s4.w, t.w);
-                }
-                *reinterpret_cast<float4*>(p.C + off) = s4;
-            } else {
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    if (c + j >= N) continue;
-                    float v = __ldcg(p.partial + off + j);
-                    for (int q = 1; q < p.splits; q++) v = __fadd_rn(v, __ldcg(p.partial + (size_t)q * MN + off + j));
-                    p.C[off + j] = v;
-                }
-            }
-        }
-    }
-    if (tid == 0) p.counters[tile] = 0u;   // leave the counter ready for the next call
+    simt_epilogue<TM, GN>(p, acc, out_row, out_col, VEC, z, tile, sm.last);
 }
 
 template <int BM, int BN, bool FUSED, bool VEC>
@@ -284,6 +302,156 @@ sgemm_simt_kernel(SimtArgs p) {
     __shared__ __align__(16) SimtSmem<BM, BN> sm;
     simt_tile<BM, BN, FUSED, VEC ? 1 : 0>(p, (int64_t)blockIdx.y * BM, (int64_t)blockIdx.x * BN, blockIdx.z,
                                           blockIdx.y * gridDim.x + blockIdx.x, sm);
+}
+
+// ---------------------------------------------------------------------------
+// 128 x 128 tiles on a cp.async pipeline (the plan's 128 x 128 FP32 tile).
+//
+// 128 threads (four warps of 64 x 64), each owning 8 x 16 outputs: rows
+// wm*64 + lm + 8i (i < 8), columns wn*64 + 4 ln + 16 j + {0..3} (j < 4), with
+// lane = 4 lm + ln. Two CTAs per SM. Tiles of A (128 rows x 32 k, row-major,
+// rows padded to 36 floats) and B (32 k x 128 columns) arrive by cp.async
+// (16-byte copies where K and N are multiples of 4 and A, B, C are 16-byte
+// aligned; 4-byte copies otherwise) into a ring of three stages, so no thread
+// stages operands through registers or transposes them. Per four k's a
+// thread reads its 8 rows of A as 128-bit loads (4 k's each; a warp's eight
+// rows fall on eight bank groups) and, per k, 16 values of B (four 128-bit
+// loads, 64 contiguous bytes per warp): 512 multiply-adds per 24 shared loads.
+//
+// Arithmetic: as in the kernel above, every output is one chain over k in
+// increasing order (the stage loop, then four k's per A load, in order), so
+// C is the same bit for bit; copies outside the matrix fill zeros.
+// ---------------------------------------------------------------------------
+namespace cpk {
+constexpr int BM = 128, BN = 128, BK = 32, STAGES = 3, THREADS = 128;
+constexpr int AST = BK + 4;                    // A row stride (floats): eight rows on eight bank groups
+constexpr int A_FLOATS = BM * AST;
+constexpr int B_FLOATS = BK * BN;
+constexpr int STAGE_FLOATS = A_FLOATS + B_FLOATS;
+constexpr int SMEM = STAGES * STAGE_FLOATS * 4;
+}  // namespace cpk
+
+__device__ __forceinline__ void cp_async_16(uint32_t dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_4(uint32_t dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+template <bool FUSED, bool VEC>
+__global__ void __launch_bounds__(cpk::THREADS, 2)
+sgemm_simt_cp_kernel(SimtArgs p) {
+    using namespace cpk;
+    extern __shared__ __align__(16) float smem[];
+    __shared__ int last_flag;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp >> 1, wn = warp & 1;
+    const int lm = lane >> 2, ln = lane & 3;
+    const int64_t m0 = (int64_t)blockIdx.y * BM, n0 = (int64_t)blockIdx.x * BN;
+    const int z = blockIdx.z;
+    const int64_t M = p.M, N = p.N, K = p.K;
+    const int64_t kbeg = (int64_t)z * p.kchunk;
+    const int64_t kend = min(K, kbeg + p.kchunk);
+    const int64_t ntiles = (kend - kbeg + BK - 1) / BK;
+    const float* __restrict__ A = p.A;
+    const float* __restrict__ B = p.B;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(smem);
+
+    // Stage `buf` <- A[m0.., k0..k0+BK), B[k0..k0+BK, n0..); zeros outside the
+    // matrix and past kend (a copy of 0 source bytes reads nothing; its source
+    // address is kept inside the operand anyway).
+    auto load_stage = [&](int buf, int64_t k0) {
+        const uint32_t a_s = sbase + (uint32_t)(buf * STAGE_FLOATS) * 4u;
+        const uint32_t b_s = a_s + (uint32_t)A_FLOATS * 4u;
+        if constexpr (VEC) {
+#pragma unroll
+            for (int j = 0; j < BM * BK / 4 / THREADS; j++) {       // 8 chunks of A
+                const int c = tid + j * THREADS;
+                const int row = c >> 3, ch = c & 7;
+                const int64_t gm = m0 + row, gk = k0 + ch * 4;
+                const bool ok = gm < M && gk < kend;
+                cp_async_16(a_s + (uint32_t)(row * AST + ch * 4) * 4u, ok ? A + gm * K + gk : A, ok ? 16 : 0);
+            }
+#pragma unroll
+            for (int j = 0; j < BK * BN / 4 / THREADS; j++) {       // 8 chunks of B
+                const int c = tid + j * THREADS;
+                const int row = c >> 5, ch = c & 31;
+                const int64_t gk = k0 + row, gn = n0 + ch * 4;
+                const bool ok = gk < kend && gn < N;
+                cp_async_16(b_s + (uint32_t)(row * BN + ch * 4) * 4u, ok ? B + gk * N + gn : B, ok ? 16 : 0);
+            }
+        } else {
+#pragma unroll 8
+            for (int j = 0; j < BM * BK / THREADS; j++) {           // 32 elements of A
+                const int c = tid + j * THREADS;
+                const int row = c >> 5, col = c & 31;
+                const int64_t gm = m0 + row, gk = k0 + col;
+                const bool ok = gm < M && gk < kend;
+                cp_async_4(a_s + (uint32_t)(row * AST + col) * 4u, ok ? A + gm * K + gk : A, ok ? 4 : 0);
+            }
+#pragma unroll 8
+            for (int j = 0; j < BK * BN / THREADS; j++) {           // 32 elements of B
+                const int c = tid + j * THREADS;
+                const int row = c >> 7, col = c & 127;
+                const int64_t gk = k0 + row, gn = n0 + col;
+                const bool ok = gk < kend && gn < N;
+                cp_async_4(b_s + (uint32_t)(row * BN + col) * 4u, ok ? B + gk * N + gn : B, ok ? 4 : 0);
+            }
+        }
+    };
+
+    float acc[8][16];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 16; j++) acc[i][j] = 0.f;
+
+#pragma unroll
+    for (int st = 0; st < STAGES - 1; st++) {
+        if (st < ntiles) load_stage(st, kbeg + (int64_t)st * BK);
+        cp_async_commit();
+    }
+    for (int64_t t = 0; t < ntiles; t++) {
+        cp_async_wait<STAGES - 2>();
+        __syncthreads();                       // stage t landed; stage t - 1 is no longer read
+        const int64_t tn = t + STAGES - 1;
+        if (tn < ntiles) load_stage((int)(tn % STAGES), kbeg + tn * BK);
+        cp_async_commit();
+        const float* As = smem + (int)(t % STAGES) * STAGE_FLOATS;
+        const float* Bs = As + A_FLOATS;
+        const float* a_base = As + (wm * 64 + lm) * AST;
+        const float* b_base = Bs + wn * 64 + ln * 4;
+#pragma unroll
+        for (int k4 = 0; k4 < BK / 4; k4++) {
+            float4 a[8];
+#pragma unroll
+            for (int i = 0; i < 8; i++) a[i] = *reinterpret_cast<const float4*>(a_base + i * 8 * AST + k4 * 4);
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++) {
+                float b[16];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const float4 v = *reinterpret_cast<const float4*>(b_base + (k4 * 4 + kk) * BN + j * 16);
+                    b[4 * j + 0] = v.x; b[4 * j + 1] = v.y; b[4 * j + 2] = v.z; b[4 * j + 3] = v.w;
+                }
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    const float av = kk == 0 ? a[i].x : kk == 1 ? a[i].y : kk == 2 ? a[i].z : a[i].w;
+#pragma unroll
+                    for (int j = 0; j < 16; j++) acc[i][j] = mac<FUSED>(av, b[j], acc[i][j]);
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+
+    // Steps past kend multiplied zeros: the chains are those over [kbeg, kend).
+    auto out_row = [&](int i) { return m0 + wm * 64 + lm + 8 * i; };
+    auto out_col = [&](int g) { return n0 + wn * 64 + ln * 4 + 16 * g; };
+    simt_epilogue<8, 4>(p, acc, out_row, out_col, VEC, z, blockIdx.y * gridDim.x + blockIdx.x, last_flag);
 }
 
 // Grouped launch: one persistent kernel over a list of (problem, tile, K
@@ -328,6 +496,27 @@ simt_splitk_reduce_kernel(const float* __restrict__ partial, float* __restrict__
 // Slices at or above which the partials are summed by the reduction kernel.
 constexpr int kReduceAfterSplits = 3;
 
+// Raises a kernel's dynamic shared memory limit once per device.
+template <typename Kern>
+cudaError_t smem_limit_once(Kern kern, int bytes, std::atomic<uint64_t>& done) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 64 && ((done.load() >> dev) & 1u)) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && dev < 64) done.fetch_or(1ull << dev);
+    return e;
+}
+
+template <bool FUSED, bool VEC>
+cudaError_t launch_cp(const SimtArgs& a, dim3 grid, cudaStream_t s) {
+    static std::atomic<uint64_t> done{0};
+    cudaError_t e = smem_limit_once(sgemm_simt_cp_kernel<FUSED, VEC>, cpk::SMEM, done);
+    if (e != cudaSuccess) return e;
+    sgemm_simt_cp_kernel<FUSED, VEC><<<grid, cpk::THREADS, cpk::SMEM, s>>>(a);
+    return cudaGetLastError();
+}
+
 template <int BM, int BN>
 cudaError_t launch_tile(const SimtArgs& args, int variant, cudaStream_t s) {
     SimtArgs a = args;
@@ -339,11 +528,18 @@ cudaError_t launch_tile(const SimtArgs& args, int variant, cudaStream_t s) {
     cudaError_t e;
     {
         PhaseScope ps(kPhaseGemm, s);
-        if (fused && vec) sgemm_simt_kernel<BM, BN, true, true><<<grid, kThreads, 0, s>>>(a);
-        else if (fused) sgemm_simt_kernel<BM, BN, true, false><<<grid, kThreads, 0, s>>>(a);
-        else if (vec) sgemm_simt_kernel<BM, BN, false, true><<<grid, kThreads, 0, s>>>(a);
-        else sgemm_simt_kernel<BM, BN, false, false><<<grid, kThreads, 0, s>>>(a);
-        e = cudaGetLastError();
+        if constexpr (BM == cpk::BM && BN == cpk::BN) {
+            if (fused && vec) e = launch_cp<true, true>(a, grid, s);
+            else if (fused) e = launch_cp<true, false>(a, grid, s);
+            else if (vec) e = launch_cp<false, true>(a, grid, s);
+            else e = launch_cp<false, false>(a, grid, s);
+        } else {
+            if (fused && vec) sgemm_simt_kernel<BM, BN, true, true><<<grid, kThreads, 0, s>>>(a);
+            else if (fused) sgemm_simt_kernel<BM, BN, true, false><<<grid, kThreads, 0, s>>>(a);
+            else if (vec) sgemm_simt_kernel<BM, BN, false, true><<<grid, kThreads, 0, s>>>(a);
+            else sgemm_simt_kernel<BM, BN, false, false><<<grid, kThreads, 0, s>>>(a);
+            e = cudaGetLastError();
+        }
     }
     if (e != cudaSuccess || !a.reduce_after) return e;
     PhaseScope ps(kPhaseReduce, s);
