@@ -875,19 +875,16 @@ struct CfgFused {
     static constexpr int RING = OP_STAGES * OP_STAGE + ST_STAGES * ST_STAGE;
     static constexpr int NPROD = (MODE == MAXMULSK_PREC_BF16X6) ? 6 : 9;
     static constexpr uint32_t IDESC = make_idesc(1u, 128u, (uint32_t)BN, 1u);
-    static constexpr int NACC = 4;                   // TMEM accumulators (4 x 128 columns)
-    static constexpr uint32_t TMEM_COLS = NACC * BN;
-    static constexpr int EPI = 8;                    // epilogue warps 2 .. 9
-    static constexpr int COLS = BN * 4 / EPI;
-    static constexpr int LDW = 32;
-    static constexpr int NCONV = 4;                  // converter warps 10 .. 13
+    static constexpr int NACC = 3;                   // TMEM accumulators (3 x 128 columns)
+    static constexpr uint32_t SUM_COL = NACC * BN;   // the unit's running sums: TMEM columns 384 .. 511
+    static constexpr uint32_t TMEM_COLS = (NACC + 1) * BN;
+    static constexpr int EPI = 4;                    // epilogue warps 2 .. 5, one per TMEM lane quarter
+    static constexpr int NCONV = 8;                  // converter warps 6 .. 13: four for A, four for B
     static constexpr int THREADS = 64 + 32 * (EPI + NCONV);
-    // Register writeback: at 448 threads the register cap is 128, and the
-    // store boxes' code made the epilogue spill (measured 2 % slower on
-    // 128 x 32768 x 512, whose C is 256 KB).
+    // C leaves from the TMEM sums 32 columns at a time through registers.
     static constexpr bool TMA_STORE = false;
-    static constexpr int SMEM = RING + 1024 + (TMA_STORE ? EPI * kStoreWarpBytes : 0);
-    static_assert(NCONV * 32 == BM && NCONV == NBOX, "one converter lane per A row and per B box row");
+    static constexpr int SMEM = RING + 1024;
+    static_assert(NCONV * 16 == BM && NCONV == 2 * NBOX, "one converter lane per A row and per B box row");
 };
 
 // Units of a grouped launch: device tables of problems, units (heaviest
@@ -928,6 +925,141 @@ struct GroupSrc {
         tmap_acquire(b);
     }
 };
+
+// Epilogue of the fused-split kernel: four warps, one per TMEM lane quarter,
+// each thread one row of the 128 x 128 tile. A unit's running sums live in
+// TMEM columns SUM_COL .. SUM_COL + 127 rather than in registers, which
+// leaves the register budget to the eight converter warps: per chunk, 32
+// columns at a time, the chunk's accumulator and the running sum are loaded,
+// added with round-to-nearest (the first chunk is copied), and the sum is
+// stored back -- the same adds, in the same order, as the register
+// epilogue's. A whole tile then leaves from TMEM 32 columns at a time; a K
+// slice writes its partial row, and the last slice to arrive on this warp's
+// counter sums every slice in slice order, 32 columns at a time.
+template <class Cf, class Src>
+__device__ __forceinline__ void epilogue_role_tsum(const Src& src, int* err, long long timeout, uint32_t tmem_base,
+                                                   uint64_t* tfull_bar, uint64_t* tempty_bar, volatile int& abort_s,
+                                                   int warp, int lane) {
+    constexpr int BN = Cf::BN;
+    constexpr int W = 32;                             // columns per TMEM load
+    auto fail = [&]() {
+        atomicOr(err, kErrTimeout);
+        abort_s = 1;
+    };
+    auto kblocks = [&](const Unit& w) -> int64_t { return (w.kend - w.kbeg + Cf::BK - 1) / Cf::BK; };
+    const int ew = warp - 2;                          // epilogue warp 0 .. EPI-1
+    const int quarter = warp & 3;                     // TMEM lanes 32*quarter .. +31
+    const uint32_t lanes = (uint32_t)(quarter * 32) << 16;
+    const uint32_t tsum = tmem_base + lanes + Cf::SUM_COL;
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    bool stop = false;
+    for (int64_t round = 0, u = src.unit_of(0); u < src.units() && !stop; u = src.unit_of(++round)) {
+        UnitView v;
+        src.get(u, v);
+        const Unit& w = v.w;
+        const int64_t M = v.M, N = v.N;
+        const bool vec = (N % 4 == 0) && ((reinterpret_cast<uintptr_t>(v.C) & 15) == 0) &&
+                         (v.partial == nullptr || (reinterpret_cast<uintptr_t>(v.partial) & 15) == 0);
+        const int64_t nkb = kblocks(w);
+        for (int64_t kb0 = 0; kb0 < nkb; kb0 += v.chunk_kb) {
+            int bad = abort_s;
+            if (!bad && lane == 0) {
+                if (!mbar_wait_bounded(&tfull_bar[acc], acc_phase, timeout)) { fail(); bad = 1; }
+            }
+            bad = __shfl_sync(0xffffffffu, bad, 0);
+            if (bad) { stop = true; break; }
+            tc_fence_after();
+            const uint32_t tacc = tmem_base + lanes + (uint32_t)(acc * BN);
+#pragma unroll
+            for (int c = 0; c < BN; c += W) {
+                uint32_t r[W];
+                tmem_ld_32x32b_x32(tacc + (uint32_t)c, r);
+                if (kb0 == 0) {
+                    tmem_wait_ld();
+                    tmem_st_32x32b_x32(tsum + (uint32_t)c, r);
+                } else {
+                    uint32_t q[W];
+                    tmem_ld_32x32b_x32(tsum + (uint32_t)c, q);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int j = 0; j < W; j++)
+                        q[j] = __float_as_uint(__fadd_rn(__uint_as_float(q[j]), __uint_as_float(r[j])));
+                    tmem_st_32x32b_x32(tsum + (uint32_t)c, q);
+                }
+            }
+            tmem_wait_st();                           // the sums are in TMEM before the next chunk reads them
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty_bar[acc]);
+            if (++acc == Cf::NACC) { acc = 0; acc_phase ^= 1u; }
+        }
+        if (stop) break;
+
+        // ---- the unit's sums are complete in TMEM: store them
+        const int lrow = quarter * 32 + lane;         // row within the tile
+        const int64_t row = (int64_t)w.tm * Cf::BM + lrow;
+        const int64_t col0 = (int64_t)w.tn * BN;
+        if (w.sti < 0) {
+#pragma unroll
+            for (int c = 0; c < BN; c += W) {
+                uint32_t q[W];
+                tmem_ld_32x32b_x32(tsum + (uint32_t)c, q);
+                tmem_wait_ld();
+                float f[W];
+#pragma unroll
+                for (int j = 0; j < W; j++) f[j] = __uint_as_float(q[j]);
+                store_row_regs<W>(f, v.C, row, col0 + c, M, N, vec);
+            }
+            continue;
+        }
+        constexpr size_t TILE = (size_t)Cf::BM * BN;
+        float* seg = v.partial + (size_t)w.sti * v.max_splits * TILE + (size_t)lrow * BN;
+        float* part = seg + (size_t)w.z * TILE;
+#pragma unroll
+        for (int c = 0; c < BN; c += W) {
+            uint32_t q[W];
+            tmem_ld_32x32b_x32(tsum + (uint32_t)c, q);
+            tmem_wait_ld();
+#pragma unroll
+            for (int j = 0; j < W; j += 4)
+                __stcg(reinterpret_cast<float4*>(part + c + j),
+                       make_float4(__uint_as_float(q[j]), __uint_as_float(q[j + 1]), __uint_as_float(q[j + 2]),
+                                   __uint_as_float(q[j + 3])));
+        }
+        if (v.reduce_after) continue;
+        unsigned* ctr = v.counters + (size_t)w.sti * Cf::EPI + ew;
+        __threadfence();
+        __syncwarp();
+        int last = 0;
+        if (lane == 0) last = (atomicAdd(ctr, 1u) == (unsigned)(w.nsplit - 1));
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (!last) continue;
+        __threadfence();
+#pragma unroll 1
+        for (int c = 0; c < BN; c += W) {
+            float sum[W];
+#pragma unroll
+            for (int j = 0; j < W; j += 4) {
+                const float4 t = __ldcg(reinterpret_cast<const float4*>(seg + c + j));
+                sum[j] = t.x; sum[j + 1] = t.y; sum[j + 2] = t.z; sum[j + 3] = t.w;
+            }
+            for (int qz = 1; qz < w.nsplit; qz++) {
+                const float* bq = seg + (size_t)qz * TILE + c;
+#pragma unroll
+                for (int j = 0; j < W; j += 4) {
+                    const float4 t = __ldcg(reinterpret_cast<const float4*>(bq + j));
+                    sum[j] = __fadd_rn(sum[j], t.x);
+                    sum[j + 1] = __fadd_rn(sum[j + 1], t.y);
+                    sum[j + 2] = __fadd_rn(sum[j + 2], t.z);
+                    sum[j + 3] = __fadd_rn(sum[j + 3], t.w);
+                }
+            }
+            store_row_regs<W>(sum, v.C, row, col0 + c, M, N, vec);
+        }
+        if (lane == 0) *ctr = 0u;
+    }
+}
 
 template <int MODE, class Src>
 __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, const void* tmB1, const void* tmC1,
@@ -1068,15 +1200,18 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
         }
     } else if (warp < CONV0) {
         // ------------------------------------------------------------ epilogue
-        uint8_t* cbuf = (Cf::TMA_STORE && tmC1) ? smem + Cf::RING + (warp - 2) * kStoreWarpBytes : nullptr;
-        epilogue_role<Cf, BN>(src, err, timeout, tmem_base, tfull_bar, tempty_bar, abort_s, warp, lane, cbuf);
+        epilogue_role_tsum<Cf>(src, err, timeout, tmem_base, tfull_bar, tempty_bar, abort_s, warp, lane);
     } else {
         // ------------------------------------------------------------ converters
-        // Warp cw splits A rows 32cw .. 32cw+31 (one per lane) and the 32 k
-        // rows of B box cw (columns 32cw .. 32cw+31), one k row per lane.
+        // Warps cw = 0..3 split A rows 32cw .. 32cw+31 (one per lane); warps
+        // 4..7 split the 32 k rows of B box cw - 4 (columns 32(cw-4) .. +31),
+        // one k row per lane: two converter warps per SM sub-partition, so one
+        // warp's shared-memory traffic overlaps the other's arithmetic.
         // Shared-memory accesses: a quarter-warp covers 8 consecutive rows,
         // whose swizzled 16-byte chunks fall on distinct banks.
-        const int cw = warp - CONV0;
+        const int cwx = warp - CONV0;
+        const bool conv_a = cwx < Cf::NCONV / 2;
+        const int cw = conv_a ? cwx : cwx - Cf::NCONV / 2;
         int stage = 0, ostage = 0;
         uint32_t phase = 0, ophase = 0;
         bool stop = false;
@@ -1097,7 +1232,7 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
                 if (bad) { stop = true; break; }
                 const uint8_t* sa = stg + (size_t)stage * Cf::ST_STAGE;
                 uint8_t* oa = ops + (size_t)ostage * Cf::OP_STAGE;
-                {
+                if (conv_a) {
                     // A row r: 32 FP32 k's (128-byte row, 128-byte swizzle) ->
                     // three 64-byte BF16 rows (64-byte swizzle).
                     const int r = cw * 32 + lane;
@@ -1117,8 +1252,7 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
                         *reinterpret_cast<uint4*>(oa + Cf::A_PLANE + off) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
                         *reinterpret_cast<uint4*>(oa + 2 * Cf::A_PLANE + off) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
                     }
-                }
-                {
+                } else {
                     // B row k of box cw: 32 FP32 n's -> four 16-byte chunks of
                     // 8 BF16 in column panel cw / 2, chunks 4 (cw % 2) .. +3.
                     const int k = lane;
