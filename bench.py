@@ -445,9 +445,11 @@ def run_tables(args) -> None:
     # split precision: the fused-split tcgen05 kernel over the group (A with K
     # not a multiple of 4 is repacked in the graph; N not a multiple of 4
     # would run in the FP32 part of the same graph)
-    for name, pc in (("bf16x6", 2), ("bf16x9", 3)):
+    for name, pc in (("bf16x6", 2), ("bf16x9", 3), ("split_auto", 4)):
         gt = mm.Grouped(probs, mm.make_plan(pc, 128, 128, 0))
         tp, tsplits, tunits = gt.info()
+        tplans = gt.plans()
+        singles = [i for i, p in enumerate(tplans) if p.precision != 0 and p.variant != mm.TC_FUSED_SPLIT]
         for _ in range(3):
             gt.launch()
         torch.cuda.synchronize()
@@ -457,17 +459,30 @@ def run_tables(args) -> None:
         e1.record()
         torch.cuda.synchronize()
         t_tc = e0.elapsed_time(e1) / 1e3 / reps
-        peak = peaks["bf16_tflops"] / PRODUCTS[pc]
         nw = []
         for i in np.random.default_rng(0).choice(len(shapes), 16, replace=False):
             a, b, c, M, K, N = probs[i]
             nw.append(mm.Fp64Check(a, b, M, K, N, with_abs=False).errors(c)["normwise"])
+        # the same problems as one launch each (the picker's plan of each
+        # problem for this precision), replayed from one CUDA graph
+        pfns, pkeep = [], []
+        for (a, b, c, M, K, N) in probs:
+            fn, ws = run_plan(a, b, c, M, K, N, mm.choose(M, K, N, pc))
+            pfns.append(fn)
+            pkeep.append(ws)
+        t_per = graph_time(torch, lambda: [f() for f in pfns], 1)
+        del pkeep
+        peak_b = peaks["bf16_tflops"] / PRODUCTS[3 if pc == 3 else 2]
         emit({"workload": "grouped", "precision": name, "problems": len(shapes), "gflop": flops / 1e9,
               "units": tunits, "fp32_fallback_problems": sum(1 for M, K, N in shapes if N % 4),
               "a_repacked_problems": sum(1 for M, K, N in shapes if K % 4 and not N % 4),
-              "plan": {"tile_m": 128, "tile_n": 128, "split_k_max": max(tsplits), "variant": "fused split"},
+              "plan": {"fused_tile": "128x128", "split_k_max": max(tsplits),
+                       "own_launch_problems": len(singles),
+                       "own_launch_gflop": sum(2.0 * shapes[i][0] * shapes[i][1] * shapes[i][2] for i in singles) / 1e9,
+                       "search": "group configurations timed at creation"},
               "grouped_ms": t_tc * 1e3, "grouped_gflops": flops / t_tc / 1e9,
-              "frac_split_roofline": flops / t_tc / 1e12 / peak,
+              "frac_split_roofline": flops / t_tc / 1e12 / peak_b,
+              "per_gemm_launches_ms": t_per * 1e3, "per_gemm_launches_gflops": flops / t_per / 1e9,
               "normwise_max_of_16_sampled": max(nw)})
         gt.close()
 

@@ -222,17 +222,25 @@ typedef struct {
 
 typedef struct maxmulsk_grouped_s* maxmulsk_grouped;
 
-/* Plans the group (tile shape for the group, K split per problem; group_plan
- * may be NULL for the picker, or an FP32 plan whose split_k is 0 = per problem
- * or > 0 = for all), uploads its tables, allocates its scratch and captures one
- * CUDA graph. Call with the device current.
- * A group_plan of precision MAXMULSK_PREC_BF16X6 / _BF16X9 / _SPLIT_AUTO
- * (= BF16X6) runs the problems on the fused-split tensor-core kernel, 128 x 128
- * tiles (tile and variant fields are ignored; split_k as for FP32). An A with
- * K not a multiple of 4 (or not 16-byte aligned) is copied to a padded buffer
- * of the group inside the graph; problems with N not a multiple of 4, or B not
- * 16-byte aligned, run in the FP32 SIMT part of the same graph, at FP32
- * accuracy. */
+/* Plans the group, uploads its tables, allocates its scratch and captures one
+ * CUDA graph. Call with the device current and the problems' buffers idle.
+ * group_plan NULL, or an FP32 plan: the FP32 grouped kernel. Its tile (one per
+ * group; NULL = chosen) and K split (split_k > 0 = that split for every
+ * problem, 0 = chosen per problem) are what the caller gives; what is left
+ * open is chosen by timing candidate configurations of the whole group (tile
+ * shape x K-split policy), each captured and replayed, the fastest kept --
+ * the group-level form of maxmulsk_autotune_dev. The search runs the group,
+ * so C is written while the group is created.
+ * A group_plan of precision MAXMULSK_PREC_BF16X6 / _BF16X9 / _SPLIT_AUTO runs
+ * the problems on the fused-split tensor-core kernel, 128 x 128 tiles (tile
+ * and variant fields are ignored). With split_k 0 the search also decides
+ * which large problems run instead as their own launches of their picked plan
+ * (split pre-pass + tcgen05 GEMM, 3xTF32 allowed under SPLIT_AUTO) inside
+ * the same graph. An A with K not a multiple of 4 (or not 16-byte aligned) is
+ * copied to a padded buffer of the group inside the graph; problems with N
+ * not a multiple of 4, or B not 16-byte aligned, run in the FP32 SIMT part of
+ * the same graph, at FP32 accuracy. maxmulsk_grouped_plans tells each
+ * problem's plan. */
 maxmulsk_status maxmulsk_grouped_create(const maxmulsk_problem* problems, size_t count,
                                         const maxmulsk_plan* group_plan, maxmulsk_grouped* out);
 /* Replays the captured graph on `stream` (asynchronous). */
@@ -241,6 +249,13 @@ maxmulsk_status maxmulsk_grouped_launch(maxmulsk_grouped g, void* stream);
  * be NULL), number of work units. */
 maxmulsk_status maxmulsk_grouped_info(maxmulsk_grouped g, maxmulsk_plan* group_plan, int32_t* split_k,
                                       size_t* units);
+/* The plan each problem runs (count entries): FP32 problems the group's tile,
+ * their K split and variant; fused problems (precision, 128, 128, K split,
+ * MAXMULSK_TC_FUSED_SPLIT) -- for an A repacked to a padded pitch the result
+ * is that of MAXMULSK_TC_SPLIT_INPUTS on the same tiles; problems run as their
+ * own launches, their plan. Each problem's C equals a single launch of its
+ * plan bit for bit. */
+maxmulsk_status maxmulsk_grouped_plans(maxmulsk_grouped g, maxmulsk_plan* plans);
 void maxmulsk_grouped_destroy(maxmulsk_grouped g);
 /* One-shot: create, launch on `stream`, wait, destroy. */
 maxmulsk_status maxmulsk_sgemm_grouped_dev(const maxmulsk_problem* problems, size_t count, void* stream);

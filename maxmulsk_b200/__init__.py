@@ -320,6 +320,12 @@ class Grouped:
         check(lib().maxmulsk_grouped_info(self.handle, ctypes.byref(p), sk, ctypes.byref(units)), "grouped_info")
         return p, list(sk)[: self.count], units.value
 
+    def plans(self) -> list:
+        """The plan each problem runs (maxmulsk_grouped_plans)."""
+        arr = (Plan * max(1, self.count))()
+        check(lib().maxmulsk_grouped_plans(self.handle, arr), "grouped_plans")
+        return [arr[i] for i in range(self.count)]
+
     def close(self):
         if getattr(self, "handle", None):
             lib().maxmulsk_grouped_destroy(self.handle)

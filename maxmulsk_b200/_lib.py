@@ -87,6 +87,7 @@ _SIGNATURES: dict[str, tuple] = {
     "maxmulsk_grouped_create": (c_int32, [POINTER(Problem), c_size_t, POINTER(Plan), POINTER(c_void_p)]),
     "maxmulsk_grouped_launch": (c_int32, [c_void_p, c_void_p]),
     "maxmulsk_grouped_info": (c_int32, [c_void_p, POINTER(Plan), POINTER(c_int32), POINTER(c_size_t)]),
+    "maxmulsk_grouped_plans": (c_int32, [c_void_p, POINTER(Plan)]),
     "maxmulsk_grouped_destroy": (None, [c_void_p]),
     "maxmulsk_sgemm_grouped_dev": (c_int32, [POINTER(Problem), c_size_t, c_void_p]),
     "maxmulsk_candidates": (c_size_t, [c_int32, POINTER(Plan), c_size_t]),

@@ -1,5 +1,7 @@
 // Grouped launches: many independent GEMMs of uneven shapes in one persistent
-// kernel, captured once into a CUDA graph and replayed.
+// kernel, captured once into a CUDA graph and replayed; how the group is cut
+// into work is chosen by timing candidate graphs (an exhaustive search over a
+// few group configurations) unless the caller fixes it.
 //
 // The reference's counterpart is run_batch (sme/v3/sme-1x4-acc-kcout-onestream.hpp:61-63,
 // .cpp:598-605): one streaming region for a list of Gemm{A, B, C, M, K, N},
@@ -16,7 +18,20 @@
 //     aligned) is copied, inside the same graph, into a zero-padded buffer of
 //     the group with rows of a multiple of 4 floats. A problem whose B cannot
 //     be read that way (N not a multiple of 4, B not 16-byte aligned) runs in
-//     the FP32 grouped kernel captured in the same graph, at FP32 accuracy.
+//     the FP32 grouped kernel captured in the same graph, at FP32 accuracy;
+//   * split-precision problems of at least `single_gflop` GFLOP whose own
+//     picked plan (tuning database, learned model, rule) is not the fused
+//     split run as their own launches of that plan (split pre-pass +
+//     tcgen05 GEMM on larger tiles) in the same graph, after the persistent
+//     kernel: a problem big enough to fill the GPU on its own gains more from
+//     its best plan than from sharing the fused kernel's 128 x 128 tiles.
+//
+// Configuration search (maxmulsk_grouped_create with no K split given): each
+// candidate -- FP32: tile shape x K-split policy; split precision: the fused
+// part's K-split policy x the single-launch threshold -- is built, captured,
+// replayed once to warm and three times timed (median), and the fastest is
+// kept: the group-level counterpart of maxmulsk_autotune_dev. It runs the
+// group, so C is written while the group is created.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -56,6 +71,15 @@ struct maxmulsk_grouped_s {
     };
     std::vector<Repack> repack;
     void* d_apad = nullptr;
+    // split-precision problems run as their own launches
+    struct Single {
+        size_t problem;
+        maxmulsk_plan plan;
+    };
+    std::vector<Single> singles;
+    void* d_single_ws = nullptr;           // shared by the singles (one after another on one stream)
+    size_t single_ws_bytes = 0;
+    std::vector<maxmulsk_plan> plans;      // per problem, as run
     // the captured graph
     cudaStream_t cap = nullptr;
     cudaGraph_t graph = nullptr;
@@ -94,14 +118,15 @@ void pick_tile(const maxmulsk_problem* probs, const std::vector<size_t>& idx, in
     }
 }
 
-// K split of each problem: units no longer than a quarter of a work slot's
+// K split of each problem: units no longer than 1/share of a work slot's
 // average share of the group, slices at least 256 deep, at most 64 slices.
-// fixed > 0 imposes that split on every problem.
+// fixed > 0 imposes that split on every problem; share <= 0 splits none.
 std::vector<int> plan_splits(const maxmulsk_problem* probs, const std::vector<size_t>& idx, int bm, int bn,
-                             int slots, int fixed) {
+                             int slots, int fixed, double share) {
     double total = 0;
     for (size_t i : idx) total += padded_work(probs[i], bm, bn);
-    const double cap = std::max(1.0, total / (4.0 * slots));
+    if (fixed <= 0 && share <= 0) return std::vector<int>(idx.size(), 1);
+    const double cap = std::max(1.0, total / (share * slots));
     std::vector<int> out(idx.size(), 1);
     for (size_t j = 0; j < idx.size(); j++) {
         const maxmulsk_problem& p = probs[idx[j]];
@@ -122,10 +147,15 @@ std::vector<int> plan_splits(const maxmulsk_problem* probs, const std::vector<si
 
 // FP32 part: the problems `idx` on the SIMT grouped kernel.
 maxmulsk_status build_simt(maxmulsk_grouped_s* g, const maxmulsk_problem* problems, const std::vector<size_t>& idx,
-                           const maxmulsk_plan& plan, int sms) {
+                           const maxmulsk_plan& plan, double share, int sms) {
     const int bm = plan.tile_m, bn = plan.tile_n;
-    const std::vector<int> sk = plan_splits(problems, idx, bm, bn, 2 * sms, plan.split_k);   // 2 CTAs per SM
-    for (size_t j = 0; j < idx.size(); j++) g->split_k[idx[j]] = sk[j];
+    const std::vector<int> sk = plan_splits(problems, idx, bm, bn, 2 * sms, plan.split_k, share);   // 2 CTAs per SM
+    for (size_t j = 0; j < idx.size(); j++) {
+        g->split_k[idx[j]] = sk[j];
+        maxmulsk_plan& q = g->plans[idx[j]];
+        q = plan;
+        q.split_k = sk[j];
+    }
 
     std::vector<GroupProblem> hp(idx.size());
     std::vector<GroupUnit> hu;
@@ -196,10 +226,15 @@ maxmulsk_status build_simt(maxmulsk_grouped_s* g, const maxmulsk_problem* proble
 
 // Split-precision part: the problems `idx` on the fused-split tcgen05 kernel.
 maxmulsk_status build_tc(maxmulsk_grouped_s* g, const maxmulsk_problem* problems, const std::vector<size_t>& idx,
-                         int precision, int fixed_split, int sms) {
+                         int precision, int fixed_split, double share, int sms) {
     constexpr int T = 128;                                    // tile rows and columns
-    const std::vector<int> sk = plan_splits(problems, idx, T, T, sms, fixed_split);   // 1 CTA per SM
+    const std::vector<int> sk = plan_splits(problems, idx, T, T, sms, fixed_split, share);   // 1 CTA per SM
     const size_t n = idx.size();
+    for (size_t j = 0; j < n; j++) {
+        maxmulsk_plan& q = g->plans[idx[j]];
+        std::memset(&q, 0, sizeof q);
+        q.precision = precision; q.tile_m = T; q.tile_n = T; q.split_k = sk[j]; q.variant = MAXMULSK_TC_FUSED_SPLIT;
+    }
     std::vector<TcGroupProblem> hp(n);
     std::vector<TcGroupUnit> hu;
     std::vector<unsigned char> maps(256 * std::max<size_t>(1, n));
@@ -312,6 +347,175 @@ bool fused_readable(const maxmulsk_problem& p) {
     return p.N % 4 == 0 && ((uintptr_t)p.B % 16) == 0;
 }
 
+// How a group is cut into work (one candidate of the configuration search).
+struct GroupConfig {
+    maxmulsk_plan simt{};          // FP32 part: tile, variant; split_k > 0 = that split for all
+    double simt_share = 4.0;       // FP32 K-split policy (plan_splits) when split_k == 0
+    int tc_precision = 0;          // 0: FP32 group; else BF16X6 / BF16X9 (the fused kernel)
+    int tc_request = 0;            // the precision asked for (SPLIT_AUTO lets singles pick 3xTF32)
+    int tc_fixed = 0;              // > 0: that split for every fused problem
+    double tc_share = 4.0;
+    double single_gflop = INFINITY;
+};
+
+// Split-precision problems that run as their own launches under `cfg`.
+void pick_singles(const maxmulsk_problem* problems, std::vector<size_t>& tc_idx, const GroupConfig& cfg, int sms,
+                  std::vector<maxmulsk_grouped_s::Single>& singles) {
+    if (!(cfg.single_gflop < INFINITY)) return;
+    std::vector<size_t> keep;
+    for (size_t i : tc_idx) {
+        const maxmulsk_problem& p = problems[i];
+        const double gflop = 2.0 * (double)p.M * (double)p.N * (double)p.K * 1e-9;
+        if (gflop >= cfg.single_gflop) {
+            const maxmulsk_plan pl = choose_tuned(p.M, p.K, p.N, cfg.tc_request, sms);
+            if (pl.precision != MAXMULSK_PREC_FP32 && pl.variant != MAXMULSK_TC_FUSED_SPLIT &&
+                classify_plan(p.M, p.K, p.N, &pl) == MAXMULSK_OK) {
+                singles.push_back({i, pl});
+                continue;
+            }
+        }
+        keep.push_back(i);
+    }
+    tc_idx.swap(keep);
+}
+
+// Plans, tables and scratch of one configuration (no capture yet).
+maxmulsk_status build_group(maxmulsk_grouped_s* g, const maxmulsk_problem* problems, size_t count,
+                            const GroupConfig& cfg, int sms) {
+    g->count = count;
+    g->split_k.assign(count, 1);
+    g->plans.assign(count, maxmulsk_plan{});
+    std::vector<size_t> simt_idx, tc_idx;
+    for (size_t i = 0; i < count; i++) {
+        if (cfg.tc_precision && runs(problems[i]) && fused_readable(problems[i])) tc_idx.push_back(i);
+        else simt_idx.push_back(i);
+    }
+    pick_singles(problems, tc_idx, cfg, sms, g->singles);
+    g->simt_plan = cfg.simt;
+    if (cfg.tc_precision) {
+        std::memset(&g->plan, 0, sizeof g->plan);
+        g->plan.precision = cfg.tc_precision; g->plan.tile_m = 128; g->plan.tile_n = 128;
+        g->plan.split_k = cfg.tc_fixed; g->plan.variant = MAXMULSK_TC_FUSED_SPLIT;
+    } else {
+        g->plan = cfg.simt;
+    }
+    maxmulsk_status st = build_simt(g, problems, simt_idx, cfg.simt, cfg.simt_share, sms);
+    if (st == MAXMULSK_OK && !tc_idx.empty())
+        st = build_tc(g, problems, tc_idx, cfg.tc_precision, cfg.tc_fixed, cfg.tc_share, sms);
+    if (st != MAXMULSK_OK) return st;
+    size_t ws = 0;
+    for (const auto& sg : g->singles) {
+        const maxmulsk_problem& p = problems[sg.problem];
+        g->plans[sg.problem] = sg.plan;
+        g->split_k[sg.problem] = sg.plan.split_k;
+        ws = std::max(ws, workspace_bytes(p.M, p.K, p.N, sg.plan));
+    }
+    if (ws) {
+        cudaError_t e = cudaMalloc(&g->d_single_ws, ws);
+        if (e != cudaSuccess) return cuda_status(e, "cudaMalloc(grouped single-launch workspace)");
+        g->single_ws_bytes = ws;
+    }
+    return MAXMULSK_OK;
+}
+
+// Captures the group's work into its graph: K == 0 problems zero-filled, the
+// unit counter and split-K arrival counters reset, the A repacks, the
+// persistent kernel(s), then the single launches.
+maxmulsk_status capture_group(maxmulsk_grouped_s* g, const maxmulsk_problem* problems) {
+    cudaError_t e = cudaStreamCreateWithFlags(&g->cap, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_status(e, "cudaStreamCreate");
+    maxmulsk_status st = MAXMULSK_OK;
+    e = cudaStreamBeginCapture(g->cap, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        for (size_t i = 0; i < g->count; i++)
+            if (problems[i].M && problems[i].N && !problems[i].K)
+                cudaMemsetAsync(problems[i].C, 0, problems[i].M * problems[i].N * sizeof(float), g->cap);
+        if (g->tc_counters && g->tc_counter_bytes) cudaMemsetAsync(g->tc_counters, 0, g->tc_counter_bytes, g->cap);
+        for (const auto& r : g->repack) {
+            cudaError_t ec = cudaMemcpy2DAsync(r.dst, r.dst_ld * sizeof(float), r.src, r.cols * sizeof(float),
+                                               r.cols * sizeof(float), r.rows, cudaMemcpyDeviceToDevice, g->cap);
+            if (ec != cudaSuccess) e = ec;
+        }
+        if (g->tc.nunits > 0) {
+            cudaError_t el = tc_grouped_launch(g->tc, g->plan.precision, g->tc_grid, g->cap);
+            if (el != cudaSuccess) e = el;
+        }
+        cudaMemsetAsync(g->d_next, 0, sizeof(unsigned), g->cap);
+        if (g->d_scratch && g->counter_bytes) cudaMemsetAsync(g->d_scratch, 0, g->counter_bytes, g->cap);
+        if (g->nunits > 0)
+            simt_grouped_launch(g->d_probs, g->d_units, g->nunits, g->d_next, g->simt_plan.tile_m,
+                                g->simt_plan.tile_n, g->simt_plan.variant, g->grid, g->cap);
+        for (const auto& sg : g->singles) {
+            const maxmulsk_problem& p = problems[sg.problem];
+            maxmulsk_status s1 = run_plan_dev(p.A, p.B, p.C, p.M, p.K, p.N, sg.plan, g->d_single_ws,
+                                              g->single_ws_bytes, g->cap);
+            if (s1 != MAXMULSK_OK && st == MAXMULSK_OK) st = s1;
+        }
+        cudaError_t e2 = cudaStreamEndCapture(g->cap, &g->graph);
+        if (e == cudaSuccess) e = e2;
+    }
+    if (e == cudaSuccess && st == MAXMULSK_OK) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    if (st != MAXMULSK_OK) return st;
+    return cuda_status(e, "grouped graph capture");
+}
+
+// Median of three timed replays of the group's graph (after one warm
+// replay), in milliseconds; +inf if a replay fails.
+float time_group(maxmulsk_grouped_s* g) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        return INFINITY;
+    }
+    float t[3] = {INFINITY, INFINITY, INFINITY};
+    cudaError_t e = cudaGraphLaunch(g->exec, g->cap);
+    for (int i = 0; i < 3 && e == cudaSuccess; i++) {
+        cudaEventRecord(e0, g->cap);
+        e = cudaGraphLaunch(g->exec, g->cap);
+        cudaEventRecord(e1, g->cap);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) cudaEventElapsedTime(&t[i], e0, e1);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess || stream_status(g->cap) != MAXMULSK_OK) return INFINITY;
+    std::sort(t, t + 3);
+    return t[1];
+}
+
+// The candidates searched when the caller leaves the cut to the library.
+std::vector<GroupConfig> candidate_configs(const GroupConfig& base, bool search_tile, bool search_simt,
+                                           bool search_tc) {
+    const int tiles[3][2] = {{128, 128}, {128, 64}, {64, 64}};
+    const double shares[4] = {0.0, 2.0, 4.0, 8.0};            // 0: no K split
+    std::vector<GroupConfig> simt_opts;
+    if (search_simt) {
+        for (int t = 0; t < (search_tile ? 3 : 1); t++)
+            for (double sh : shares) {
+                GroupConfig c = base;
+                if (search_tile) { c.simt.tile_m = tiles[t][0]; c.simt.tile_n = tiles[t][1]; }
+                c.simt_share = sh;
+                simt_opts.push_back(c);
+            }
+    } else {
+        simt_opts.push_back(base);
+    }
+    if (!base.tc_precision || !search_tc) return simt_opts;
+    // Split-precision groups: the FP32 part (problems the fused split cannot
+    // read) keeps the first option; the search runs over the rest.
+    std::vector<GroupConfig> out;
+    const double tc_shares[3] = {2.0, 4.0, 8.0};
+    const double singles[4] = {INFINITY, 32.0, 8.0, 2.0};
+    for (double th : singles)
+        for (double sh : tc_shares) {
+            GroupConfig c = simt_opts.front();
+            c.tc_share = sh;
+            c.single_gflop = th;
+            out.push_back(c);
+        }
+    return out;
+}
+
 }  // namespace
 }  // namespace mmsk
 
@@ -335,91 +539,75 @@ maxmulsk_status maxmulsk_grouped_create(const maxmulsk_problem* problems, size_t
             return MAXMULSK_ERR_UNSUPPORTED;
         }
     }
-    maxmulsk_plan plan;
-    std::memset(&plan, 0, sizeof plan);
-    plan.precision = MAXMULSK_PREC_FP32;
-    int tc_precision = 0;
+    GroupConfig base;
+    std::memset(&base.simt, 0, sizeof base.simt);
+    base.simt.precision = MAXMULSK_PREC_FP32;
+    base.simt.variant = MAXMULSK_FP32_FMA;
+    bool search_tile = true, search_simt = true, search_tc = false;
+    const int sms = device_sm_count() > 0 ? device_sm_count() : 148;
+    std::vector<size_t> all(count);
+    for (size_t i = 0; i < count; i++) all[i] = i;
     if (group_plan) {
-        plan = *group_plan;
-        if (plan.precision == MAXMULSK_PREC_SPLIT_AUTO) plan.precision = MAXMULSK_PREC_BF16X6;
-        if (plan.precision == MAXMULSK_PREC_BF16X6 || plan.precision == MAXMULSK_PREC_BF16X9) {
-            tc_precision = plan.precision;
-            plan.tile_m = 128; plan.tile_n = 128; plan.variant = MAXMULSK_TC_FUSED_SPLIT;
-            if (plan.split_k < 0 || plan.split_k > 64) {
-                set_error_message("split_k must be 0 (per problem) or 1..64");
-                return MAXMULSK_ERR_UNSUPPORTED;
-            }
+        const maxmulsk_plan plan = *group_plan;
+        if (plan.split_k < 0 || plan.split_k > 64) {
+            set_error_message("split_k must be 0 (chosen by the library) or 1..64");
+            return MAXMULSK_ERR_UNSUPPORTED;
+        }
+        if (plan.precision == MAXMULSK_PREC_SPLIT_AUTO || plan.precision == MAXMULSK_PREC_BF16X6 ||
+            plan.precision == MAXMULSK_PREC_BF16X9) {
+            base.tc_request = plan.precision;
+            base.tc_precision = plan.precision == MAXMULSK_PREC_BF16X9 ? MAXMULSK_PREC_BF16X9 : MAXMULSK_PREC_BF16X6;
+            base.tc_fixed = plan.split_k;
+            search_tc = plan.split_k == 0;
+            // problems the fused split cannot read: FP32, tile by padded work, split by the formula
+            std::vector<size_t> fp32_idx;
+            for (size_t i = 0; i < count; i++)
+                if (!(runs(problems[i]) && fused_readable(problems[i]))) fp32_idx.push_back(i);
+            pick_tile(problems, fp32_idx, &base.simt.tile_m, &base.simt.tile_n);
+            search_tile = search_simt = false;
         } else if (plan.precision != MAXMULSK_PREC_FP32) {
-            set_error_message("grouped launches run FP32, BF16X6 or BF16X9 plans");
+            set_error_message("grouped launches run FP32, BF16X6, BF16X9 or SPLIT_AUTO plans");
             return MAXMULSK_ERR_UNSUPPORTED;
         } else {
             maxmulsk_plan probe = plan;
-            if (probe.split_k == 0) probe.split_k = 1;        // 0 = per problem, picked here
+            if (probe.split_k == 0) probe.split_k = 1;
             maxmulsk_status st = classify_plan(1, 1, 1, &probe);
             if (st != MAXMULSK_OK) return st;
+            base.simt.tile_m = plan.tile_m; base.simt.tile_n = plan.tile_n; base.simt.variant = plan.variant;
+            base.simt.split_k = plan.split_k;
+            search_tile = false;
+            search_simt = plan.split_k == 0;
+        }
+    } else {
+        pick_tile(problems, all, &base.simt.tile_m, &base.simt.tile_n);
+    }
+
+    const std::vector<GroupConfig> cands = candidate_configs(base, search_tile, search_simt, search_tc);
+    std::unique_ptr<maxmulsk_grouped_s> best;
+    float best_ms = INFINITY;
+    maxmulsk_status last = MAXMULSK_OK;
+    for (const GroupConfig& cfg : cands) {
+        std::unique_ptr<maxmulsk_grouped_s> g(new (std::nothrow) maxmulsk_grouped_s());
+        if (!g) return MAXMULSK_ERR_ALLOC;
+        cudaGetDevice(&g->device);
+        maxmulsk_status st = build_group(g.get(), problems, count, cfg, sms);
+        if (st == MAXMULSK_OK) st = capture_group(g.get(), problems);
+        if (st != MAXMULSK_OK) {
+            last = st;
+            maxmulsk_grouped_destroy(g.release());
+            continue;
+        }
+        const float ms = cands.size() > 1 ? time_group(g.get()) : 0.0f;
+        if (!best || ms < best_ms) {
+            if (best) maxmulsk_grouped_destroy(best.release());
+            best = std::move(g);
+            best_ms = ms;
+        } else {
+            maxmulsk_grouped_destroy(g.release());
         }
     }
-
-    std::unique_ptr<maxmulsk_grouped_s> g(new (std::nothrow) maxmulsk_grouped_s());
-    if (!g) return MAXMULSK_ERR_ALLOC;
-    cudaGetDevice(&g->device);
-    g->count = count;
-    g->split_k.assign(count, 1);
-    const int sms = device_sm_count() > 0 ? device_sm_count() : 148;
-
-    std::vector<size_t> simt_idx, tc_idx;
-    for (size_t i = 0; i < count; i++) {
-        if (tc_precision && runs(problems[i]) && fused_readable(problems[i])) tc_idx.push_back(i);
-        else simt_idx.push_back(i);
-    }
-    maxmulsk_plan simt_plan = plan;
-    if (tc_precision || !group_plan) {
-        simt_plan.precision = MAXMULSK_PREC_FP32;
-        simt_plan.variant = MAXMULSK_FP32_FMA;
-        simt_plan.split_k = tc_precision ? 0 : plan.split_k;
-        pick_tile(problems, simt_idx, &simt_plan.tile_m, &simt_plan.tile_n);
-    }
-    if (!tc_precision) plan = simt_plan;
-    g->plan = plan;
-    g->simt_plan = simt_plan;
-
-    maxmulsk_status st = build_simt(g.get(), problems, simt_idx, simt_plan, sms);
-    if (st == MAXMULSK_OK && !tc_idx.empty()) st = build_tc(g.get(), problems, tc_idx, tc_precision, plan.split_k, sms);
-    if (st != MAXMULSK_OK) { maxmulsk_grouped_destroy(g.release()); return st; }
-
-    // Capture: K == 0 problems are zero-filled; the unit counter and the
-    // split-K arrival counters are reset; then the persistent kernel(s).
-    cudaError_t e = cudaStreamCreateWithFlags(&g->cap, cudaStreamNonBlocking);
-    if (e != cudaSuccess) { maxmulsk_grouped_destroy(g.release()); return cuda_status(e, "cudaStreamCreate"); }
-    e = cudaStreamBeginCapture(g->cap, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-        for (size_t i = 0; i < count; i++)
-            if (problems[i].M && problems[i].N && !problems[i].K)
-                cudaMemsetAsync(problems[i].C, 0, problems[i].M * problems[i].N * sizeof(float), g->cap);
-        if (g->tc_counters && g->tc_counter_bytes) cudaMemsetAsync(g->tc_counters, 0, g->tc_counter_bytes, g->cap);
-        for (const auto& r : g->repack) {
-            cudaError_t ec = cudaMemcpy2DAsync(r.dst, r.dst_ld * sizeof(float), r.src, r.cols * sizeof(float),
-                                               r.cols * sizeof(float), r.rows, cudaMemcpyDeviceToDevice, g->cap);
-            if (ec != cudaSuccess) e = ec;
-        }
-        if (g->tc.nunits > 0) {
-            cudaError_t el = tc_grouped_launch(g->tc, tc_precision, g->tc_grid, g->cap);
-            if (el != cudaSuccess) e = el;
-        }
-        cudaMemsetAsync(g->d_next, 0, sizeof(unsigned), g->cap);
-        if (g->d_scratch && g->counter_bytes) cudaMemsetAsync(g->d_scratch, 0, g->counter_bytes, g->cap);
-        if (g->nunits > 0)
-            simt_grouped_launch(g->d_probs, g->d_units, g->nunits, g->d_next, simt_plan.tile_m, simt_plan.tile_n,
-                                simt_plan.variant, g->grid, g->cap);
-        cudaError_t e2 = cudaStreamEndCapture(g->cap, &g->graph);
-        if (e == cudaSuccess) e = e2;
-    }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
-    if (e != cudaSuccess) {
-        maxmulsk_grouped_destroy(g.release());
-        return cuda_status(e, "grouped graph capture");
-    }
-    *out = g.release();
+    if (!best) return last != MAXMULSK_OK ? last : MAXMULSK_ERR_UNSUPPORTED;
+    *out = best.release();
     return MAXMULSK_OK;
 }
 
@@ -434,7 +622,13 @@ maxmulsk_status maxmulsk_grouped_info(maxmulsk_grouped g, maxmulsk_plan* group_p
     if (!g) return MAXMULSK_ERR_INVALID;
     if (group_plan) *group_plan = g->plan;
     if (split_k) std::memcpy(split_k, g->split_k.data(), g->count * sizeof(int32_t));
-    if (units) *units = (size_t)g->nunits + (size_t)g->tc.nunits;
+    if (units) *units = (size_t)g->nunits + (size_t)g->tc.nunits + g->singles.size();
+    return MAXMULSK_OK;
+}
+
+maxmulsk_status maxmulsk_grouped_plans(maxmulsk_grouped g, maxmulsk_plan* plans) {
+    if (!g || (!plans && g->count)) return MAXMULSK_ERR_INVALID;
+    if (g->count) std::memcpy(plans, g->plans.data(), g->count * sizeof(maxmulsk_plan));
     return MAXMULSK_OK;
 }
 
@@ -449,6 +643,7 @@ void maxmulsk_grouped_destroy(maxmulsk_grouped g) {
     cudaFree(g->d_scratch);
     cudaFree(g->d_tc);
     cudaFree(g->d_apad);
+    cudaFree(g->d_single_ws);
     delete g;
 }
 

@@ -35,6 +35,9 @@ def _group(cuda, oracle_mod, shapes, seed, plan=None):
 
 def _check(cuda, oracle_mod, g, cbuf, host, offs, shapes):
     plan, splits, _ = g.info()
+    plans = g.plans()
+    assert [p.split_k for p in plans] == list(splits)
+    assert all(p.precision == 0 and (p.tile_m, p.tile_n) == (plan.tile_m, plan.tile_n) for p in plans)
     c = cbuf.cpu().numpy()
     mask = np.ones(c.size, bool)
     for (M, K, N), (A, B), off, s in zip(shapes, host, offs, splits):
@@ -135,11 +138,12 @@ def test_grouped_split_precision_matches_single_launches(cuda, oracle_mod, prec)
     g, cbuf, host, offs = _group(cuda, oracle_mod, MIXED_TC, 700, mm.make_plan(prec, 128, 128, 0))
     plan, splits, units = g.info()
     assert plan.precision == int(prec) and plan.variant == mm.TC_FUSED_SPLIT and units > 0
+    plans = g.plans()
     assert g.launch() == 0
     assert mm.stream_status() == 0
     c = cbuf.cpu().numpy()
     mask = np.ones(c.size, bool)
-    for (M, K, N), (A, B), off, s in zip(MIXED_TC, host, offs, splits):
+    for (M, K, N), (A, B), off, p in zip(MIXED_TC, host, offs, plans):
         got = c[off: off + M * N].reshape(M, N)
         mask[off: off + M * N] = False
         if M * N == 0:
@@ -147,13 +151,16 @@ def test_grouped_split_precision_matches_single_launches(cuda, oracle_mod, prec)
         if K == 0:
             assert np.all(got == 0)
             continue
-        if N % 4 == 0:
-            variant = mm.TC_FUSED_SPLIT if K % 4 == 0 else mm.TC_SPLIT_INPUTS
-            st, want, _ = run_plan(cuda, A, B, M, K, N, mm.make_plan(prec, 128, 128, s, variant))
+        if p.precision != 0:
+            want_plan = p
+            if p.variant == mm.TC_FUSED_SPLIT and K % 4:
+                want_plan = mm.make_plan(p.precision, 128, 128, p.split_k, mm.TC_SPLIT_INPUTS)
+            st, want, _ = run_plan(cuda, A, B, M, K, N, want_plan)
             assert st == 0
         else:
-            want = oracle_mod.sgemm_panels(A, B, M, K, N, kc=mm.slice_len(K, s), fma=True)
-        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), ((M, K, N), s)
+            assert N % 4 != 0
+            want = oracle_mod.sgemm_panels(A, B, M, K, N, kc=mm.slice_len(K, p.split_k), fma=True)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), ((M, K, N), p)
     assert np.all(c[mask] == SENT), "a grouped launch wrote outside its C matrices"
     # replays reproduce the result
     first = cbuf.clone()
@@ -189,3 +196,26 @@ def test_grouped_benchmark_batch_split_precision(cuda):
     for c in Cs:
         assert not bool(torch.isnan(c).any())
     g.close()
+
+
+def test_grouped_split_precision_big_problems_run_their_own_plans(cuda, oracle_mod):
+    # A group with problems large enough to fill the GPU on their own: the
+    # configuration search may run them as their own launches of their picked
+    # plan inside the graph. Whatever it picks, every problem equals a single
+    # launch of the plan maxmulsk_grouped_plans reports, bit for bit, and a
+    # fixed split forces every problem onto the fused kernel.
+    shapes = [(512, 4096, 3072), (384, 8192, 2048), (33, 2048, 512), (7, 512, 1024), (200, 1000, 2048),
+              (129, 4096, 1024)]
+    g, cbuf, host, offs = _group(cuda, oracle_mod, shapes, 900, mm.make_plan(mm.Precision.SPLIT_AUTO, 128, 128, 0))
+    plans = g.plans()
+    assert g.launch() == 0 and mm.stream_status() == 0
+    c = cbuf.cpu().numpy()
+    for (M, K, N), (A, B), off, p in zip(shapes, host, offs, plans):
+        assert p.precision in (1, 2)
+        st, want, _ = run_plan(cuda, A, B, M, K, N, p)
+        assert st == 0
+        assert np.array_equal(c[off: off + M * N].view(np.uint32), want.ravel().view(np.uint32)), ((M, K, N), p)
+    g.close()
+    g2, _, _, _ = _group(cuda, oracle_mod, shapes, 900, mm.make_plan(mm.Precision.BF16X6, 128, 128, 3))
+    assert all(p.variant == mm.TC_FUSED_SPLIT and p.split_k == 3 for p in g2.plans())
+    g2.close()
