@@ -15,7 +15,16 @@ def pinning_inputs(rng, M, K, N, mode, side, level):
     cancel exactly and C = sum over pairs of (residual limbs of A) * B; side "b"
     the same with the roles of A and B swapped. All products of one limb pair
     have the same magnitude, and every partial sum fits in 24 bits, so any
-    order of accumulation gives the exact value."""
+    order of accumulation gives the exact value.
+
+    Only the last MMA k-step of each 32-k accumulation chunk (16 k's for
+    BF16, 8 for TF32) holds pairs; every other k is zero. Measured on B200:
+    an MMA aligns its sum to its largest product, cancelling ones included,
+    so an MMA of unit-size products issued after smaller terms in the same
+    accumulator truncates them below about 2^-24 (BF16x9's three extra
+    products, 2^-26 below the leading one, vanished that way). With the
+    pairs in the chunk's last k-step, the leading limbs' MMAs meet a zero
+    accumulator, and the chunk sums are added in FP32 registers."""
     tf32 = int(mode) == 1
     d = [2.0 ** -12] if tf32 else [2.0 ** -9, 2.0 ** -17]
 
@@ -45,4 +54,8 @@ def pinning_inputs(rng, M, K, N, mode, side, level):
         B[0::2, :], B[1::2, :] = y, -lead
         x = any_vals(M * half).reshape(M, half)
         A[:, 0::2], A[:, 1::2] = x, x
+    kstep = 8 if tf32 else 16
+    active = (np.arange(K) % 32) >= 32 - kstep
+    A[:, ~active] = 0.0
+    B[~active, :] = 0.0
     return A.ravel(), B.ravel()
