@@ -116,14 +116,22 @@ enum {
  *               (sme/v3/sme-1x4-acc-kcout.cpp:464-471, 530-558).
  *   variant   : FP32: MAXMULSK_FP32_FMA or MAXMULSK_FP32_SCALAR.
  *               Tensor cores: MAXMULSK_TC_SPLIT_INPUTS, MAXMULSK_TC_REUSE_PLANES or
- *               MAXMULSK_TC_FUSED_SPLIT. */
+ *               MAXMULSK_TC_FUSED_SPLIT.
+ *   chunk     : tensor cores only: k's accumulated in TMEM before the epilogue
+ *               adds them into FP32 registers (round to nearest, in k order) --
+ *               the counterpart of the reference's Kc panel, whose partial
+ *               products are added into C panel after panel. A multiple of 32
+ *               in 32 .. 4096; 0 = chosen by K (shorter chunks cost more
+ *               drains and give less error). FP32 plans: 0.
+ *   reserved  : zero. */
 typedef struct {
     int32_t precision;
     int32_t tile_m;
     int32_t tile_n;
     int32_t split_k;
     int32_t variant;
-    int32_t reserved[3];
+    int32_t chunk;
+    int32_t reserved[2];
 } maxmulsk_plan;
 
 /* Validates a plan for a shape (the analog of NB::classify,

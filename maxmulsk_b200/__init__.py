@@ -160,9 +160,10 @@ def sgemm_split_dev(dA, dB, dC, M: int, K: int, N: int, precision: int = Precisi
 
 # --------------------------------------------------------------------------- plans
 def make_plan(precision: int = Precision.FP32, tile_m: int = 128, tile_n: int = 128, split_k: int = 1,
-              variant: int = 0) -> Plan:
+              variant: int = 0, chunk: int = 0) -> Plan:
     p = Plan()
     p.precision, p.tile_m, p.tile_n, p.split_k, p.variant = int(precision), tile_m, tile_n, split_k, variant
+    p.chunk = chunk
     return p
 
 

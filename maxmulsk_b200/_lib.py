@@ -22,12 +22,14 @@ class Plan(ctypes.Structure):
         ("tile_n", c_int32),
         ("split_k", c_int32),
         ("variant", c_int32),
-        ("reserved", c_int32 * 3),
+        ("chunk", c_int32),
+        ("reserved", c_int32 * 2),
     ]
 
     def __repr__(self) -> str:
         return (f"Plan(precision={self.precision}, tile_m={self.tile_m}, tile_n={self.tile_n}, "
-                f"split_k={self.split_k}, variant={self.variant})")
+                f"split_k={self.split_k}, variant={self.variant}"
+                + (f", chunk={self.chunk})" if self.chunk else ")"))
 
     def as_tuple(self) -> tuple[int, int, int, int, int]:
         return (self.precision, self.tile_m, self.tile_n, self.split_k, self.variant)

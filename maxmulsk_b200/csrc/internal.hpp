@@ -80,6 +80,7 @@ struct TcArgs {
     int tile_m;            // 128 (one CTA per tile) or 256 (a CTA pair per tile)
     int tile_n;            // 64, 128 or 256
     int split_k;           // the plan's split_k
+    int chunk;             // k's per TMEM accumulation, 0 = chunk_len's choice
     bool reuse_planes;     // skip the split pre-pass: planes are already in place
     bool fused;            // split inside the GEMM kernel (BF16 modes, 128 x 128 tiles)
     void* planes;          // operand planes written by the split pre-pass

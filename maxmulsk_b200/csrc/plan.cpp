@@ -44,6 +44,7 @@ maxmulsk_status classify_plan(size_t M, size_t K, size_t N, const maxmulsk_plan*
         }
         if (M > kMaxDim || N > kMaxDim || K > kMaxDim) { set_error_message("dimension too large"); return MAXMULSK_ERR_UNSUPPORTED; }
         if ((M + p.tile_m - 1) / p.tile_m > 65535) { set_error_message("M too large for the FP32 grid"); return MAXMULSK_ERR_UNSUPPORTED; }
+        if (p.chunk != 0) { set_error_message("FP32 plans take chunk 0"); return MAXMULSK_ERR_UNSUPPORTED; }
         return MAXMULSK_OK;
     }
     if (is_tc(p.precision)) {
@@ -65,6 +66,10 @@ maxmulsk_status classify_plan(size_t M, size_t K, size_t N, const maxmulsk_plan*
         }
         if (M > kMaxDim || N > kMaxDim || K > kMaxDim) { set_error_message("dimension too large"); return MAXMULSK_ERR_UNSUPPORTED; }
         if (N > 32ull * 65535ull) { set_error_message("N too large for the split pre-pass grid"); return MAXMULSK_ERR_UNSUPPORTED; }
+        if (p.chunk != 0 && (p.chunk < 32 || p.chunk > 4096 || p.chunk % 32 != 0)) {
+            set_error_message("chunk must be 0 or a multiple of 32 in 32 .. 4096");
+            return MAXMULSK_ERR_UNSUPPORTED;
+        }
         return MAXMULSK_OK;
     }
     set_error_message("unknown precision");
@@ -119,18 +124,19 @@ maxmulsk_plan choose_rule(size_t M, size_t K, size_t N, int precision, int sms) 
     return p;
 }
 
-// MAXMULSK_CONFIG="precision,tile_m,tile_n,split_k[,variant]" overrides the
+// MAXMULSK_CONFIG="precision,tile_m,tile_n,split_k[,variant[,chunk]]" overrides the
 // picker; malformed values are ignored, as the reference's parse_env does.
 bool parse_config_env(maxmulsk_plan& out) {
     const char* s = std::getenv("MAXMULSK_CONFIG");
     if (!s || !*s) return false;
-    int prec = 0, tm = 0, tn = 0, sk = 0, var = 0;
-    const int n = std::sscanf(s, "%d,%d,%d,%d,%d", &prec, &tm, &tn, &sk, &var);
-    if (n != 4 && n != 5) return false;
-    if (tm <= 0 || tn <= 0 || sk <= 0) return false;
+    int prec = 0, tm = 0, tn = 0, sk = 0, var = 0, chunk = 0;
+    const int n = std::sscanf(s, "%d,%d,%d,%d,%d,%d", &prec, &tm, &tn, &sk, &var, &chunk);
+    if (n < 4) return false;
+    if (tm <= 0 || tn <= 0 || sk <= 0 || chunk < 0) return false;
     maxmulsk_plan p;
     std::memset(&p, 0, sizeof(p));
-    p.precision = prec; p.tile_m = tm; p.tile_n = tn; p.split_k = sk; p.variant = (n == 5) ? var : 0;
+    p.precision = prec; p.tile_m = tm; p.tile_n = tn; p.split_k = sk; p.variant = (n >= 5) ? var : 0;
+    p.chunk = (n >= 6) ? chunk : 0;
     out = p;
     return true;
 }

@@ -148,6 +148,7 @@ maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t
     a.fused = plan.variant == MAXMULSK_TC_FUSED_SPLIT && (reinterpret_cast<uintptr_t>(dA) & 15) == 0 &&
               (reinterpret_cast<uintptr_t>(dB) & 15) == 0 && b_planes == nullptr;
     a.split_k = plan.split_k;
+    a.chunk = plan.chunk;
     a.err = ds->err_word;
     a.b_planes = a.reuse_planes ? nullptr : b_planes;
     if (!tc_bind_workspace(a, ws, ws_bytes)) {

@@ -424,7 +424,9 @@ sgemm_simt_cp_kernel(SimtArgs p) {
         const float* Bs = As + A_FLOATS;
         const float* a_base = As + (wm * 64 + lm) * AST;
         const float* b_base = Bs + wn * 64 + ln * 4;
-#pragma unroll
+        // Two of the eight four-k groups per loop body: the fully unrolled
+        // stage (4096 multiply-adds) outgrows the instruction cache.
+#pragma unroll 2
         for (int k4 = 0; k4 < BK / 4; k4++) {
             float4 a[8];
 #pragma unroll

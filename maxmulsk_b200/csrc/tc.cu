@@ -1447,7 +1447,7 @@ TcParams make_params(const TcArgs& a, const Sched& sc, int bk) {
     prm.main_kchunk = sc.main_kchunk;
     prm.tail_kchunk = sc.tail_kchunk;
     prm.max_splits = sc.max_splits;
-    prm.chunk_kb = chunk_len(a.K, sc.main_splits) / bk;
+    prm.chunk_kb = (a.chunk > 0 ? a.chunk : chunk_len(a.K, sc.main_splits)) / bk;
     prm.reduce_after = (sc.main_splits >= kReduceAfterSplits) ? 1 : 0;
     prm.store_c = 0;
     prm.C = a.C;
