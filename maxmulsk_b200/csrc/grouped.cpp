@@ -278,9 +278,6 @@ maxmulsk_status build_tc(maxmulsk_grouped_s* g, const maxmulsk_problem* problems
             g->repack.push_back({dst, p.A, p.M, p.K, (size_t)lda});
             a = dst;
         }
-        hp[j].A = a;
-        hp[j].B = p.B;
-        hp[j].lda = lda;
         if (!tc_fused_maps(a, lda, p.B, (int64_t)p.M, (int64_t)p.K, (int64_t)p.N, &maps[256 * j])) {
             set_error_message("grouped: tensor map encoding failed");
             return MAXMULSK_ERR_CUDA;
@@ -292,11 +289,7 @@ maxmulsk_status build_tc(maxmulsk_grouped_s* g, const maxmulsk_problem* problems
     for (size_t j = 0; j < n; j++) {
         const maxmulsk_problem& p = problems[idx[j]];
         TcGroupProblem& q = hp[j];
-        const float* qa = q.A;
-        const float* qb = q.B;
-        const int64_t qlda = q.lda;
         std::memset(&q, 0, sizeof q);
-        q.A = qa; q.B = qb; q.lda = qlda;
         q.M = (int64_t)p.M; q.K = (int64_t)p.K; q.N = (int64_t)p.N;
         q.C = p.C;
         q.splits = slice_count(p.K, sk[j]);

@@ -101,9 +101,6 @@ cudaError_t tc_launch(const TcArgs& a, cudaStream_t s);
 // Grouped split-precision launch (fused split kernel over many GEMMs).
 struct TcGroupProblem {
     int64_t M, K, N;
-    const float* A;        // FP32 A (or its repacked copy), rows lda floats apart
-    const float* B;        // FP32 B, rows N floats apart
-    int64_t lda;
     float* C;
     float* partial;        // split problems: [tile][slice][128 x 128] floats
     unsigned* counters;    // split problems: 8 per tile (zero on entry)

@@ -80,12 +80,6 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, uint64_
 // Shared -> global through a tensor map; the box is clipped at the tensor's
 // extent, so a partial tile never writes outside the matrix. Completion is
 // tracked per issuing thread by bulk async-groups.
-// Prefetch of a 2-D box into L2 through a tensor map (no shared memory, no
-// completion to wait for).
-__device__ __forceinline__ void tma_prefetch_l2_2d(const void* tmap, int32_t c0, int32_t c1) {
-    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];"
-                 :: "l"(reinterpret_cast<uint64_t>(tmap)), "r"(c0), "r"(c1) : "memory");
-}
 __device__ __forceinline__ void tma_store_2d(const void* tmap, const void* src, int32_t c0, int32_t c1) {
     asm volatile(
         "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];"

@@ -144,8 +144,6 @@ struct TcParams {
     int reduce_after;        // split tiles only write partials; tc_splitk_reduce_kernel sums them
     int store_c;             // whole tiles leave through the C tensor map (TMA stores)
     float* C;
-    const float* A;          // the FP32 operands (read by the fused split)
-    const float* B;
     float* partial;          // [split tile][slice][128 x BN], split tiles only
     unsigned* counters;      // EPI per split tile (one per epilogue warp)
     int* err;
@@ -203,9 +201,6 @@ struct UnitView {
     Unit w;
     int problem;             // index in a grouped launch (0 for one GEMM)
     int64_t M, N;
-    const float* A;          // FP32 operands (the fused split reads them): A rows lda floats apart,
-    const float* B;          // B rows N floats apart
-    int64_t lda;
     float* C;
     float* partial;          // the problem's partial tiles: [split tile][slice][128 x BN]
     unsigned* counters;      // the problem's arrival counters: EPI per split tile
@@ -226,7 +221,6 @@ struct SingleSrc {
         v.w = decode_unit(p, u);
         v.problem = 0;
         v.M = p.M; v.N = p.N; v.C = p.C; v.partial = p.partial; v.counters = p.counters;
-        v.A = p.A; v.B = p.B; v.lda = p.K;
         v.max_splits = p.max_splits; v.chunk_kb = p.chunk_kb; v.reduce_after = p.reduce_after;
     }
     __device__ __forceinline__ const void* map_a(const UnitView&, const void* single) const { return single; }
@@ -872,9 +866,13 @@ struct CfgFused {
     static constexpr int A_PLANE = BM * 64;          // 8 KB per A plane
     static constexpr int B_PLANE = BK * BN * ES;     // 8 KB per B plane: 2 panels of 32 k x 128 bytes
     static constexpr int OP_STAGE = P * (A_PLANE + B_PLANE);
-    static constexpr int OP_STAGES = 4;              // the FP32 tiles come to registers, not through a ring
-    static constexpr int NBOX = BN / 32;             // 32-column B boxes (one converter warp each)
-    static constexpr int RING = OP_STAGES * OP_STAGE;
+    static constexpr int OP_STAGES = 2;
+    static constexpr int ST_A = BM * BK * 4;         // FP32 A box: 128 rows x 128 bytes
+    static constexpr int ST_BOX = BK * 32 * 4;       // FP32 B box: 32 k x 32 n
+    static constexpr int NBOX = BN / 32;
+    static constexpr int ST_STAGE = ST_A + NBOX * ST_BOX;
+    static constexpr int ST_STAGES = 3;
+    static constexpr int RING = OP_STAGES * OP_STAGE + ST_STAGES * ST_STAGE;
     static constexpr int NPROD = (MODE == MAXMULSK_PREC_BF16X6) ? 6 : 9;
     static constexpr uint32_t IDESC = make_idesc(1u, 128u, (uint32_t)BN, 1u);
     static constexpr int NACC = 3;                   // TMEM accumulators (3 x 128 columns)
@@ -914,7 +912,6 @@ struct GroupSrc {
         v.w.sti = P.splits > 1 ? (int64_t)gu.tm * P.tiles_n + gu.tn : -1;
         v.problem = gu.problem;
         v.M = P.M; v.N = P.N; v.C = P.C; v.partial = P.partial; v.counters = P.counters;
-        v.A = P.A; v.B = P.B; v.lda = P.lda;
         v.max_splits = P.splits; v.chunk_kb = P.chunk_kb; v.reduce_after = 0;
     }
     __device__ __forceinline__ const void* map_a(const UnitView& v, const void*) const {
@@ -1070,6 +1067,8 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
     using Cf = CfgFused<MODE>;
     constexpr int BN = Cf::BN;
     extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t st_full[Cf::ST_STAGES];
+    __shared__ __align__(8) uint64_t st_empty[Cf::ST_STAGES];
     __shared__ __align__(8) uint64_t op_full[Cf::OP_STAGES];
     __shared__ __align__(8) uint64_t op_empty[Cf::OP_STAGES];
     __shared__ __align__(8) uint64_t tfull_bar[Cf::NACC];
@@ -1080,11 +1079,13 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
 
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* ops = smem;                                        // operand ring (1024-aligned stages)
+    uint8_t* stg = smem + Cf::OP_STAGES * Cf::OP_STAGE;         // staging ring
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     constexpr int CONV0 = 2 + Cf::EPI;                          // first converter warp
 
     if (threadIdx.x == 0) {
+        for (int s = 0; s < Cf::ST_STAGES; s++) { mbar_init(&st_full[s], 1); mbar_init(&st_empty[s], Cf::NCONV); }
         for (int s = 0; s < Cf::OP_STAGES; s++) { mbar_init(&op_full[s], Cf::NCONV); mbar_init(&op_empty[s], 1); }
         for (int a = 0; a < Cf::NACC; a++) { mbar_init(&tfull_bar[a], 1); mbar_init(&tempty_bar[a], Cf::EPI); }
         mbar_init(&done_bar, 1);
@@ -1109,7 +1110,46 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
     };
     auto kblocks = [&](const Unit& w) -> int64_t { return (w.kend - w.kbeg + Cf::BK - 1) / Cf::BK; };
 
-    if (warp == 1) {
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer (FP32 tiles)
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int64_t issued = 0;
+            for (int64_t round = 0, u = src.unit_of(0); u < src.units() && !abort_s; u = src.unit_of(++round)) {
+                UnitView v;
+                src.get(u, v);
+                const Unit& w = v.w;
+                const void* mapA = src.map_a(v, tmA1);
+                const void* mapB = src.map_b(v, tmB1);
+                src.acquire(mapA, mapB);
+                const int64_t nkb = kblocks(w);
+                bool ok = true;
+                for (int64_t kb = 0; kb < nkb; kb++) {
+                    if (!mbar_wait_bounded(&st_empty[stage], phase ^ 1u, timeout)) { fail(); ok = false; break; }
+                    if (abort_s) { ok = false; break; }
+                    uint8_t* sa = stg + (size_t)stage * Cf::ST_STAGE;
+                    mbar_arrive_expect_tx(&st_full[stage], (uint32_t)Cf::ST_STAGE);
+                    const int32_t k = (int32_t)(w.kbeg + kb * Cf::BK);
+                    tma_load_2d(sa, mapA, &st_full[stage], k, w.tm * Cf::BM);
+#pragma unroll
+                    for (int b = 0; b < Cf::NBOX; b++)
+                        tma_load_2d(sa + Cf::ST_A + b * Cf::ST_BOX, mapB, &st_full[stage], w.tn * BN + 32 * b, k);
+                    issued++;
+                    if (++stage == Cf::ST_STAGES) { stage = 0; phase ^= 1u; }
+                }
+                if (!ok) break;
+            }
+            // No copy may still be landing in shared memory when the CTA exits.
+            const int64_t first = issued > Cf::ST_STAGES ? issued - Cf::ST_STAGES : 0;
+            for (int64_t j = first; j < issued; j++) {
+                if (!mbar_wait_bounded(&st_full[j % Cf::ST_STAGES], (uint32_t)((j / Cf::ST_STAGES) & 1), timeout)) {
+                    atomicOr(err, kErrTimeout);
+                    abort_s = 1;
+                }
+            }
+        }
+    } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
         if (lane == 0) {
             int stage = 0;
@@ -1158,155 +1198,93 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
             tc_commit(&done_bar);
             if (!mbar_wait_bounded(&done_bar, 0u, timeout)) { atomicOr(err, kErrTimeout); abort_s = 1; }
         }
-    } else if (warp >= 2 && warp < CONV0) {
+    } else if (warp < CONV0) {
         // ------------------------------------------------------------ epilogue
         epilogue_role_tsum<Cf>(src, err, timeout, tmem_base, tfull_bar, tempty_bar, abort_s, warp, lane);
-    } else if (warp >= CONV0) {
+    } else {
         // ------------------------------------------------------------ converters
         // Warps cw = 0..3 split A rows 32cw .. 32cw+31 (one per lane); warps
-        // 4..7 split the 32 k rows of B's 32-column box cw - 4 (columns
-        // 32(cw-4) .. +31 of the tile), one k row per lane. Each lane loads its
-        // 32 FP32 values (128 contiguous bytes) straight into registers with
-        // 128-bit loads, one stage ahead of the stage it converts, while lane
-        // 0 has the tile's tensor-memory-access unit prefetch the FP32 box of
-        // the stage kPrefetch ahead into L2. The FP32 tiles never pass through
-        // shared memory, whose bandwidth the MMAs' operand reads already use
-        // up on 128 x 128 tiles; only the limb planes are written there.
-        // Zeros outside the matrix and past the slice, as TMA would fill.
-        constexpr int kPrefetch = 4;
+        // 4..7 split the 32 k rows of B box cw - 4 (columns 32(cw-4) .. +31),
+        // one k row per lane: two converter warps per SM sub-partition, so one
+        // warp's shared-memory traffic overlaps the other's arithmetic.
+        // Shared-memory accesses: a quarter-warp covers 8 consecutive rows,
+        // whose swizzled 16-byte chunks fall on distinct banks.
         const int cwx = warp - CONV0;
         const bool conv_a = cwx < Cf::NCONV / 2;
         const int cw = conv_a ? cwx : cwx - Cf::NCONV / 2;
-
-        // A cursor over this CTA's (unit, k stage) sequence.
-        struct Cursor {
-            int64_t round, u, kb, nkb;
+        int stage = 0, ostage = 0;
+        uint32_t phase = 0, ophase = 0;
+        bool stop = false;
+        for (int64_t round = 0, u = src.unit_of(0); u < src.units() && !stop; u = src.unit_of(++round)) {
             UnitView v;
-            bool valid;
-        };
-        auto start = [&](Cursor& c) {
-            c.round = 0;
-            c.u = src.unit_of(0);
-            c.kb = 0;
-            c.valid = c.u < src.units();
-            if (c.valid) { src.get(c.u, c.v); c.nkb = kblocks(c.v.w); }
-        };
-        auto advance = [&](Cursor& c) {
-            if (!c.valid) return;
-            if (++c.kb < c.nkb) return;
-            c.kb = 0;
-            c.u = src.unit_of(++c.round);
-            c.valid = c.u < src.units();
-            if (c.valid) { src.get(c.u, c.v); c.nkb = kblocks(c.v.w); }
-        };
-        // This lane's 32 values of the stage at `c`.
-        auto load = [&](const Cursor& c, float4 (&x)[8]) {
-#pragma unroll
-            for (int q = 0; q < 8; q++) x[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (!c.valid) return;
-            const Unit& w = c.v.w;
-            const int64_t k0 = w.kbeg + c.kb * Cf::BK;
-            if (conv_a) {
-                const int64_t gm = (int64_t)w.tm * Cf::BM + cw * 32 + lane;
-                if (gm >= c.v.M) return;
-                const float* row = c.v.A + gm * c.v.lda + k0;
-#pragma unroll
-                for (int q = 0; q < 8; q++)
-                    if (k0 + 4 * q < w.kend) x[q] = __ldg(reinterpret_cast<const float4*>(row + 4 * q));
-            } else {
-                const int64_t gk = k0 + lane;
-                if (gk >= w.kend) return;
-                const int64_t n0 = (int64_t)w.tn * BN + 32 * cw;
-                const float* row = c.v.B + gk * c.v.N + n0;
-#pragma unroll
-                for (int q = 0; q < 8; q++)
-                    if (n0 + 4 * q < c.v.N) x[q] = __ldg(reinterpret_cast<const float4*>(row + 4 * q));
-            }
-        };
-        // The FP32 box of the stage at `c` into L2 (lane 0).
-        const void* pf_maps[2] = {nullptr, nullptr};
-        int64_t pf_unit = -1;
-        auto prefetch = [&](const Cursor& c) {
-            if (!c.valid || lane != 0) return;
-            const Unit& w = c.v.w;
-            const void* map = conv_a ? src.map_a(c.v, tmA1) : src.map_b(c.v, tmB1);
-            if (c.u != pf_unit) {
-                pf_unit = c.u;
-                pf_maps[0] = src.map_a(c.v, tmA1);
-                pf_maps[1] = src.map_b(c.v, tmB1);
-                src.acquire(pf_maps[0], pf_maps[1]);
-            }
-            const int32_t k = (int32_t)(w.kbeg + c.kb * Cf::BK);
-            if (conv_a) {
-                if (cw == 0) tma_prefetch_l2_2d(map, k, w.tm * Cf::BM);
-            } else {
-                tma_prefetch_l2_2d(map, w.tn * BN + 32 * cw, k);
-            }
-        };
-
-        Cursor cur, pf;
-        start(cur);
-        start(pf);
-        for (int j = 0; j < kPrefetch; j++) { prefetch(pf); advance(pf); }
-        float4 nx[8];
-        load(cur, nx);
-        int ostage = 0;
-        uint32_t ophase = 0;
-        while (cur.valid) {
-            float4 x[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++) x[q] = nx[q];
-            Cursor nxt = cur;
-            advance(nxt);
-            load(nxt, nx);                             // the next stage's loads overlap this one
-            prefetch(pf);
-            advance(pf);
-            int bad = abort_s;
-            if (!bad && lane == 0) {
-                if (!mbar_wait_bounded(&op_empty[ostage], ophase ^ 1u, timeout)) { fail(); bad = 1; }
-            }
-            bad = __shfl_sync(0xffffffffu, bad, 0);
-            if (bad) break;
-            uint8_t* oa = ops + (size_t)ostage * Cf::OP_STAGE;
-            if (conv_a) {
-                // A row r: 32 FP32 k's -> three 64-byte BF16 rows (64-byte swizzle).
-                const int r = cw * 32 + lane;
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const float e[8] = {x[2 * j].x, x[2 * j].y, x[2 * j].z, x[2 * j].w,
-                                        x[2 * j + 1].x, x[2 * j + 1].y, x[2 * j + 1].z, x[2 * j + 1].w};
-                    uint32_t l0[4], l1[4], l2[4];
-#pragma unroll
-                    for (int q = 0; q < 4; q++) bf16_limbs2(e[2 * q], e[2 * q + 1], l0[q], l1[q], l2[q]);
-                    const int off = r * 64 + ((j ^ ((r >> 1) & 3)) << 4);
-                    *reinterpret_cast<uint4*>(oa + off) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
-                    *reinterpret_cast<uint4*>(oa + Cf::A_PLANE + off) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
-                    *reinterpret_cast<uint4*>(oa + 2 * Cf::A_PLANE + off) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
+            src.get(u, v);
+            const int64_t nkb = kblocks(v.w);
+            for (int64_t kb = 0; kb < nkb; kb++) {
+                int bad = abort_s;
+                if (!bad && lane == 0) {
+                    if (!mbar_wait_bounded(&op_empty[ostage], ophase ^ 1u, timeout) ||
+                        !mbar_wait_bounded(&st_full[stage], phase, timeout)) {
+                        fail();
+                        bad = 1;
+                    }
                 }
-            } else {
-                // B row k of box cw: 32 FP32 n's -> four 16-byte chunks of
-                // 8 BF16 in column panel cw / 2, chunks 4 (cw % 2) .. +3.
-                const int k = lane;
-                uint8_t* ob = oa + Cf::P * Cf::A_PLANE + (cw >> 1) * (Cf::BK * 128) + k * 128;
+                bad = __shfl_sync(0xffffffffu, bad, 0);
+                if (bad) { stop = true; break; }
+                const uint8_t* sa = stg + (size_t)stage * Cf::ST_STAGE;
+                uint8_t* oa = ops + (size_t)ostage * Cf::OP_STAGE;
+                if (conv_a) {
+                    // A row r: 32 FP32 k's (128-byte row, 128-byte swizzle) ->
+                    // three 64-byte BF16 rows (64-byte swizzle).
+                    const int r = cw * 32 + lane;
+                    float x[32];
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const float e[8] = {x[2 * j].x, x[2 * j].y, x[2 * j].z, x[2 * j].w,
-                                        x[2 * j + 1].x, x[2 * j + 1].y, x[2 * j + 1].z, x[2 * j + 1].w};
-                    uint32_t l0[4], l1[4], l2[4];
+                    for (int c = 0; c < 8; c++) {
+                        const float4 v = *reinterpret_cast<const float4*>(sa + r * 128 + ((c ^ (r & 7)) << 4));
+                        x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
+                    }
 #pragma unroll
-                    for (int q = 0; q < 4; q++) bf16_limbs2(e[2 * q], e[2 * q + 1], l0[q], l1[q], l2[q]);
-                    const int off = ((((cw & 1) * 4 + j) ^ (k & 7)) << 4);
-                    *reinterpret_cast<uint4*>(ob + off) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
-                    *reinterpret_cast<uint4*>(ob + Cf::B_PLANE + off) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
-                    *reinterpret_cast<uint4*>(ob + 2 * Cf::B_PLANE + off) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
+                    for (int j = 0; j < 4; j++) {
+                        uint32_t l0[4], l1[4], l2[4];
+#pragma unroll
+                        for (int e = 0; e < 4; e++) bf16_limbs2(x[8 * j + 2 * e], x[8 * j + 2 * e + 1], l0[e], l1[e], l2[e]);
+                        const int off = r * 64 + ((j ^ ((r >> 1) & 3)) << 4);
+                        *reinterpret_cast<uint4*>(oa + off) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
+                        *reinterpret_cast<uint4*>(oa + Cf::A_PLANE + off) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
+                        *reinterpret_cast<uint4*>(oa + 2 * Cf::A_PLANE + off) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
+                    }
+                } else {
+                    // B row k of box cw: 32 FP32 n's -> four 16-byte chunks of
+                    // 8 BF16 in column panel cw / 2, chunks 4 (cw % 2) .. +3.
+                    const int k = lane;
+                    const uint8_t* sb = sa + Cf::ST_A + cw * Cf::ST_BOX;
+                    float x[32];
+#pragma unroll
+                    for (int c = 0; c < 8; c++) {
+                        const float4 v = *reinterpret_cast<const float4*>(sb + k * 128 + ((c ^ (k & 7)) << 4));
+                        x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
+                    }
+                    uint8_t* ob = oa + Cf::P * Cf::A_PLANE + (cw >> 1) * (Cf::BK * 128) + k * 128;
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        uint32_t l0[4], l1[4], l2[4];
+#pragma unroll
+                        for (int e = 0; e < 4; e++) bf16_limbs2(x[8 * j + 2 * e], x[8 * j + 2 * e + 1], l0[e], l1[e], l2[e]);
+                        const int off = ((((cw & 1) * 4 + j) ^ (k & 7)) << 4);
+                        *reinterpret_cast<uint4*>(ob + off) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
+                        *reinterpret_cast<uint4*>(ob + Cf::B_PLANE + off) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
+                        *reinterpret_cast<uint4*>(ob + 2 * Cf::B_PLANE + off) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
+                    }
                 }
+                // The planes are read by the tensor cores (async proxy).
+                fence_proxy_async();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&op_full[ostage]);
+                    mbar_arrive(&st_empty[stage]);
+                }
+                if (++stage == Cf::ST_STAGES) { stage = 0; phase ^= 1u; }
+                if (++ostage == Cf::OP_STAGES) { ostage = 0; ophase ^= 1u; }
             }
-            // The planes are read by the tensor cores (async proxy).
-            fence_proxy_async();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&op_full[ostage]);
-            if (++ostage == Cf::OP_STAGES) { ostage = 0; ophase ^= 1u; }
-            cur = nxt;
         }
     }
 
@@ -1473,8 +1451,6 @@ TcParams make_params(const TcArgs& a, const Sched& sc, int bk) {
     prm.reduce_after = (sc.main_splits >= kReduceAfterSplits) ? 1 : 0;
     prm.store_c = 0;
     prm.C = a.C;
-    prm.A = a.A;
-    prm.B = a.B;
     prm.partial = a.partial;
     prm.counters = a.counters;
     prm.err = a.err;
