@@ -601,15 +601,16 @@ def main() -> None:
     # warm-up, untimed; every mode meets the accuracy bar at this shape).
     if args.precision == "auto":
         # The modes are within a few per cent of each other at this shape:
-        # three rounds over all of them, each mode's best round decides.
+        # five interleaved rounds of 100 steps over all of them, each mode's
+        # best round decides.
         steps = {name: mode_step(pc, dC) for name, pc in PREC.items()}
         for fn, _, _ in steps.values():
             for _ in range(3):
                 fn()
         best_t = {name: float("inf") for name in steps}
-        for _ in range(3):
+        for _ in range(5):
             for name, (fn, _, _) in steps.items():
-                best_t[name] = min(best_t[name], timed(fn, 30))
+                best_t[name] = min(best_t[name], timed(fn, 100))
         args.precision = min(best_t, key=best_t.get)
         del steps
     prec = 0 if args.precision == "fp32" else PREC[args.precision]

@@ -12,8 +12,8 @@
 // accumulation step, so the error of one long TMEM accumulation grows with its
 // length (measured on B200: about 0.4 * L / sqrt(K) times the FP32 SIMT
 // kernel's normwise error for a chain of L k's). The kernel therefore
-// accumulates only a short chunk of k's in TMEM at a time (32, 64 or 128 by
-// K: chunk_len); the epilogue warps add each chunk into FP32 registers, round
+// accumulates only a short chunk of k's in TMEM at a time (32, 128 or 256 by
+// K: chunk_len, or the plan's chunk); the epilogue warps add each chunk into FP32 registers, round
 // to nearest, chunk after chunk in k order. This is the reference's outer-Kc
 // panel scheme (first panel stores, later panels add:
 // sme/v3/sme-1x4-acc-kcout.cpp:464-471, :530-558) with a short panel, and it
@@ -1406,16 +1406,19 @@ Sched make_sched(int64_t M, int64_t K, int64_t N, int tile_m, int tile_n, int sp
 
 // K per TMEM accumulation chunk. Measured on B200: the split product's
 // normwise error grows with the chunk (at 4096^3, U[-1,1): 0.31x / 0.47x /
-// 0.84x / 1.6x the FP32 SIMT kernel's for 32 / 64 / 128 / 256) and is up to
-// 1.8x larger, relative to SIMT, for wide exponent ranges and small K; each
-// chunk costs one TMEM drain. Tiers that keep every measured cell at or below
-// about 1.2x SIMT: 32 below K = 4096, 64 below 16384, 128 above. A K-split
-// plan is compared against a K-split SIMT plan (shorter chains, smaller
-// error), so it keeps 32.
+// 0.84x / 1.6x the plain FP32 kernel's for 32 / 64 / 128 / 256; wide exponent
+// ranges about 1.65x more, relative), and falls with K relative to the plain
+// kernel, whose single chain lengthens with K (128 x 32768 x 512, N(0, 1/K):
+// 0.53x at 256). Each chunk costs one TMEM drain: at 4096^3 the CTA-pair
+// GEMM ran 592 us with chunks of 64 and 507 us with 256, and narrow K-split
+// plans 13 % faster with 256 than with 32. Tiers by K that keep every
+// benchmark cell within the 2x bar with room: 32 below K = 4096, 128 below
+// 16384, 256 above; a K-split plan takes the tier of its whole K (its chains
+// are no longer than an unsplit plan's).
 int chunk_len(int64_t K, int splits) {
-    if (splits > 1) return 32;
-    if (K >= 16384) return 128;
-    if (K >= 4096) return 64;
+    (void)splits;
+    if (K >= 16384) return 256;
+    if (K >= 4096) return 128;
     return 32;
 }
 
