@@ -91,7 +91,8 @@ struct TcArgs {
     int* err;              // device error word
 };
 size_t tc_workspace_bytes(int64_t M, int64_t K, int64_t N, int precision, int tile_m, int tile_n, int split_k);
-// Bytes of the arrival counters at the start of the partial area (to zero).
+// Bytes of the arrival counters at the start of the partial area to zero
+// before a launch (0 when the plan's slices are summed by a reduce kernel).
 size_t tc_counter_bytes(int64_t M, int64_t K, int64_t N, int precision, int tile_m, int tile_n, int split_k);
 // Concurrently resident work slots (SMs, or CTA pairs for 256-row tiles).
 int tc_slots(int precision, int tile_m, int tile_n);

@@ -158,8 +158,10 @@ maxmulsk_status run_plan_dev(const float* dA, const float* dB, float* dC, size_t
     if (a.counters) {
         const size_t cb = tc_counter_bytes((int64_t)M, (int64_t)K, (int64_t)N, plan.precision, plan.tile_m,
                                          plan.tile_n, plan.split_k);
-        st = cuda_status(cudaMemsetAsync(a.counters, 0, cb, s), "cudaMemsetAsync(counters)");
-        if (st != MAXMULSK_OK) return st;
+        if (cb > 0) {
+            st = cuda_status(cudaMemsetAsync(a.counters, 0, cb, s), "cudaMemsetAsync(counters)");
+            if (st != MAXMULSK_OK) return st;
+        }
     }
     return cuda_status(tc_launch(a, s), "sgemm_split_tc launch");
 }

@@ -608,8 +608,9 @@ maxmulsk_status simt_run(const float* dA, const float* dB, float* dC, size_t M, 
         set_error_message("workspace too small for the SIMT plan");
         return MAXMULSK_ERR_INVALID;
     }
-    if (a.splits > 1) {
-        // The split-K arrival counters must start at zero on every call.
+    if (a.splits > 1 && a.splits < kReduceAfterSplits) {
+        // The split-K arrival counters must start at zero on every call (with
+        // more slices, simt_splitk_reduce_kernel sums them and no counter is read).
         const size_t tiles = (size_t)((M + plan.tile_m - 1) / plan.tile_m) * ((N + plan.tile_n - 1) / plan.tile_n);
         maxmulsk_status st =
             cuda_status(cudaMemsetAsync(a.counters, 0, tiles * sizeof(unsigned), s), "cudaMemsetAsync(counters)");

@@ -1746,8 +1746,11 @@ size_t tc_workspace_bytes(int64_t M, int64_t K, int64_t N, int precision, int ti
     return align256((size_t)g.P * (g.a_plane_bytes + g.b_plane_bytes)) + partial_bytes(sc, tile_n);
 }
 
+// Counter bytes to clear before a launch: none when tc_splitk_reduce_kernel
+// sums the slices (no counter is read), which saves a launch on K-split plans.
 size_t tc_counter_bytes(int64_t M, int64_t K, int64_t N, int precision, int tile_m, int tile_n, int split_k) {
-    return counter_bytes(make_sched(M, K, N, tile_m, tile_n, split_k, tc_slots(precision, tile_m, tile_n)));
+    const Sched sc = make_sched(M, K, N, tile_m, tile_n, split_k, tc_slots(precision, tile_m, tile_n));
+    return sc.main_splits >= kReduceAfterSplits ? 0 : counter_bytes(sc);
 }
 
 bool tc_bind_workspace(TcArgs& a, void* ws, size_t ws_bytes) {
