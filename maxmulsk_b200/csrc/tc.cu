@@ -157,42 +157,51 @@ struct Unit {
 };
 
 // Tile t -> (tile row, tile column), rastered in groups of 8 tile rows so
-// concurrently running CTAs share A rows and B columns in L2.
-__device__ __forceinline__ void tile_coords(const TcParams& p, int64_t t, int& tm, int& tn) {
-    constexpr int G = 8;
-    const int64_t per_group = (int64_t)G * p.tiles_n;
-    const int64_t g = t / per_group;
-    const int64_t first_m = g * G;
-    const int64_t gsz = min((int64_t)G, (int64_t)p.tiles_m - first_m);
-    const int64_t r = t % per_group;
+// concurrently running CTAs share A rows and B columns in L2. I is the index
+// type: 32-bit unsigned division is a few instructions, 64-bit division a
+// long software routine at the start of every unit.
+template <typename I>
+__device__ __forceinline__ void tile_coords_t(const TcParams& p, I t, int& tm, int& tn) {
+    constexpr I G = 8;
+    const I per_group = G * (I)p.tiles_n;
+    const I g = t / per_group;
+    const I first_m = g * G;
+    const I gsz = min(G, (I)p.tiles_m - first_m);
+    const I r = t % per_group;
     tm = (int)(first_m + r % gsz);
     tn = (int)(r / gsz);
+}
+
+template <typename I>
+__device__ __forceinline__ Unit decode_unit_t(const TcParams& p, I u) {
+    Unit w;
+    I t;
+    int64_t kc;
+    if (u < (I)p.main_units) {
+        w.z = (int)(u % (I)p.main_splits);
+        t = u / (I)p.main_splits;
+        w.nsplit = p.main_splits;
+        kc = p.main_kchunk;
+        w.sti = (p.main_splits > 1) ? (int64_t)t : -1;
+    } else {
+        const I v = u - (I)p.main_units;
+        w.z = (int)(v % (I)p.tail_splits);
+        t = (I)p.main_tiles + v / (I)p.tail_splits;
+        w.nsplit = p.tail_splits;
+        kc = p.tail_kchunk;
+        w.sti = (p.tail_splits > 1) ? (int64_t)(t - (I)p.main_tiles) : -1;
+    }
+    w.kbeg = (int64_t)w.z * kc;
+    w.kend = min(p.K, w.kbeg + kc);
+    tile_coords_t<I>(p, t, w.tm, w.tn);
+    return w;
 }
 
 // Unit -> its tile, K slice and where its partial goes. Slices of one tile
 // are adjacent so they run at the same time.
 __device__ __forceinline__ Unit decode_unit(const TcParams& p, int64_t u) {
-    Unit w;
-    int64_t t;
-    int64_t kc;
-    if (u < p.main_units) {
-        w.z = (int)(u % p.main_splits);
-        t = u / p.main_splits;
-        w.nsplit = p.main_splits;
-        kc = p.main_kchunk;
-        w.sti = (p.main_splits > 1) ? t : -1;
-    } else {
-        const int64_t v = u - p.main_units;
-        w.z = (int)(v % p.tail_splits);
-        t = p.main_tiles + v / p.tail_splits;
-        w.nsplit = p.tail_splits;
-        kc = p.tail_kchunk;
-        w.sti = (p.tail_splits > 1) ? t - p.main_tiles : -1;
-    }
-    w.kbeg = (int64_t)w.z * kc;
-    w.kend = min(p.K, w.kbeg + kc);
-    tile_coords(p, t, w.tm, w.tn);
-    return w;
+    if (p.units <= (int64_t)UINT32_MAX) return decode_unit_t<uint32_t>(p, (uint32_t)u);
+    return decode_unit_t<uint64_t>(p, (uint64_t)u);
 }
 
 // What the roles of a persistent kernel need to know about one work unit:
@@ -844,13 +853,17 @@ cudaError_t set_smem_once(Kern kern, int bytes, std::atomic<uint64_t>& done) {
 // Fused-split variant (BF16x6 / BF16x9, 128 x 128 tiles). The operands are
 // split inside the kernel instead of by the pre-pass. Warp 0 loads FP32 tiles
 // of A (128 rows x 32 k) and B (32 k x 128 n, as four 32-column boxes) with
-// TMA and the 128-byte swizzle into a staging ring; four converter warps cut
-// each staged element into its three BF16 limbs (split_math.cuh, the
-// pre-pass's arithmetic) and write the limb planes into an operand ring in
-// the layouts the MMA reads -- the bytes TMA writes for the pre-pass planes:
-// A K-major with 64-byte rows and the 64-byte swizzle, B in 128-byte column
-// panels with the 128-byte swizzle. The MMA warp and the epilogue are those
-// of the one-CTA kernel, so C is the same bit for bit as with the pre-pass.
+// TMA and the 128-byte swizzle into a staging ring, a few stages after an L2
+// prefetch of the same boxes; eight converter warps cut each staged element
+// into its three BF16 limbs (split_math.cuh, the pre-pass's arithmetic). A's
+// limbs go to tensor memory, one row per TMEM lane, where the MMA reads them
+// as its A operand; B's limb planes go to an operand ring in shared memory in
+// the layout TMA writes for the pre-pass planes (128-byte column panels, the
+// 128-byte swizzle). Keeping A out of shared memory takes its plane stores and
+// the MMA's A reads (a third of the CTA's shared-memory traffic per stage) off
+// the shared-memory pipe, which the MMA, TMA and the converters otherwise
+// saturate on these 128-column tiles. The products, their order and the
+// epilogue are those of the one-CTA kernel.
 // Each FP32 element crosses HBM once per tile that reads it instead of being
 // read, written as planes and read again: the gain where the pre-pass costs
 // as much as the products (narrow M or N).
@@ -863,27 +876,32 @@ struct CfgFused {
     static constexpr int BK = 32;                    // k per stage: one 64-byte row of BF16
     static constexpr int KSTEP = 16;
     static constexpr int KSTEPS = BK / KSTEP;
-    static constexpr int A_PLANE = BM * 64;          // 8 KB per A plane
     static constexpr int B_PLANE = BK * BN * ES;     // 8 KB per B plane: 2 panels of 32 k x 128 bytes
-    static constexpr int OP_STAGE = P * (A_PLANE + B_PLANE);
+    static constexpr int OP_STAGE = P * B_PLANE;     // B's limb planes; A's limbs are in TMEM
     static constexpr int OP_STAGES = 2;
     static constexpr int ST_A = BM * BK * 4;         // FP32 A box: 128 rows x 128 bytes
     static constexpr int ST_BOX = BK * 32 * 4;       // FP32 B box: 32 k x 32 n
     static constexpr int NBOX = BN / 32;
     static constexpr int ST_STAGE = ST_A + NBOX * ST_BOX;
-    static constexpr int ST_STAGES = 3;
+    static constexpr int ST_STAGES = 5;
+    static constexpr int PREFETCH = 6;               // stages between a box's L2 prefetch and its load
+    static_assert(PREFETCH >= ST_STAGES, "prefetches run ahead of the staging ring");
     static constexpr int RING = OP_STAGES * OP_STAGE + ST_STAGES * ST_STAGE;
     static constexpr int NPROD = (MODE == MAXMULSK_PREC_BF16X6) ? 6 : 9;
     static constexpr uint32_t IDESC = make_idesc(1u, 128u, (uint32_t)BN, 1u);
-    static constexpr int NACC = 3;                   // TMEM accumulators (3 x 128 columns)
-    static constexpr uint32_t SUM_COL = NACC * BN;   // the unit's running sums: TMEM columns 384 .. 511
-    static constexpr uint32_t TMEM_COLS = (NACC + 1) * BN;
+    static constexpr int NACC = 2;                   // TMEM accumulators: columns 0 .. 255
+    static constexpr uint32_t SUM_COL = NACC * BN;   // the unit's running sums: columns 256 .. 383
+    static constexpr uint32_t A_COL = SUM_COL + BN;  // A's limbs: columns 384 .. 479
+    static constexpr uint32_t A_SLOT = P * BK / 2;   // 48 columns per operand stage: limb p at 16 p
+    static constexpr uint32_t TMEM_COLS = 512;
+    static_assert(A_COL + OP_STAGES * A_SLOT <= TMEM_COLS, "TMEM columns");
     static constexpr int EPI = 4;                    // epilogue warps 2 .. 5, one per TMEM lane quarter
     static constexpr int NCONV = 8;                  // converter warps 6 .. 13: four for A, four for B
     static constexpr int THREADS = 64 + 32 * (EPI + NCONV);
     // C leaves from the TMEM sums 32 columns at a time through registers.
     static constexpr bool TMA_STORE = false;
     static constexpr int SMEM = RING + 1024;
+    static_assert(SMEM <= kSmemCap, "shared memory");
     static_assert(NCONV * 16 == BM && NCONV == 2 * NBOX, "one converter lane per A row and per B box row");
 };
 
@@ -1124,6 +1142,16 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
                 const void* mapB = src.map_b(v, tmB1);
                 src.acquire(mapA, mapB);
                 const int64_t nkb = kblocks(w);
+                // The FP32 boxes of stage j go to L2 PREFETCH stages before
+                // their load, which then waits for L2 instead of HBM. The
+                // first stages are loaded at once (their loads go to HBM
+                // themselves); each prefetch follows a load.
+                auto prefetch = [&](int64_t j) {
+                    const int32_t k = (int32_t)(w.kbeg + j * Cf::BK);
+                    tma_prefetch_l2_2d(mapA, k, w.tm * Cf::BM);
+#pragma unroll
+                    for (int b = 0; b < Cf::NBOX; b++) tma_prefetch_l2_2d(mapB, w.tn * BN + 32 * b, k);
+                };
                 bool ok = true;
                 for (int64_t kb = 0; kb < nkb; kb++) {
                     if (!mbar_wait_bounded(&st_empty[stage], phase ^ 1u, timeout)) { fail(); ok = false; break; }
@@ -1135,6 +1163,9 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
 #pragma unroll
                     for (int b = 0; b < Cf::NBOX; b++)
                         tma_load_2d(sa + Cf::ST_A + b * Cf::ST_BOX, mapB, &st_full[stage], w.tn * BN + 32 * b, k);
+                    // Stages the ring does not hold yet: prefetched behind this load.
+                    for (int64_t j = (kb == 0 ? Cf::ST_STAGES : kb + Cf::PREFETCH); j <= kb + Cf::PREFETCH && j < nkb; j++)
+                        prefetch(j);
                     issued++;
                     if (++stage == Cf::ST_STAGES) { stage = 0; phase ^= 1u; }
                 }
@@ -1169,21 +1200,20 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
                     for (int64_t kb = kb0; kb < kb1; kb++) {
                         if (!mbar_wait_bounded(&op_full[stage], phase, timeout)) { fail(); ok = false; break; }
                         tc_fence_after();
-                        const uint32_t a_base = smem_u32(ops + (size_t)stage * Cf::OP_STAGE);
-                        const uint32_t b_base = a_base + Cf::P * Cf::A_PLANE;
+                        const uint32_t a_tm = tmem_base + Cf::A_COL + (uint32_t)stage * Cf::A_SLOT;
+                        const uint32_t b_base = smem_u32(ops + (size_t)stage * Cf::OP_STAGE);
 #pragma unroll
                         for (int ks = 0; ks < Cf::KSTEPS; ks++) {
 #pragma unroll
                             for (int q = 0; q < Cf::NPROD; q++) {
                                 int pa, pb;
                                 product_planes(MODE, q, pa, pb);
-                                const uint64_t adesc =
-                                    make_smem_desc(a_base + (uint32_t)(pa * Cf::A_PLANE + ks * 32), 16u, 512u, 4u);
+                                const uint32_t a_addr = a_tm + (uint32_t)(pa * (Cf::BK / 2) + ks * (Cf::KSTEP / 2));
                                 const uint64_t bdesc =
                                     make_smem_desc(b_base + (uint32_t)(pb * Cf::B_PLANE + ks * Cf::KSTEP * 128),
                                                    (uint32_t)(Cf::BK * 128), 1024u, 2u);
                                 const uint32_t accum = (kb > kb0 || ks > 0 || q > 0) ? 1u : 0u;
-                                mma_bf16(d_tmem, adesc, bdesc, Cf::IDESC, accum);
+                                mma_bf16_ta(d_tmem, a_addr, bdesc, Cf::IDESC, accum);
                             }
                         }
                         tc_commit(&op_empty[stage]);
@@ -1203,12 +1233,13 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
         epilogue_role_tsum<Cf>(src, err, timeout, tmem_base, tfull_bar, tempty_bar, abort_s, warp, lane);
     } else {
         // ------------------------------------------------------------ converters
-        // Warps cw = 0..3 split A rows 32cw .. 32cw+31 (one per lane); warps
-        // 4..7 split the 32 k rows of B box cw - 4 (columns 32(cw-4) .. +31),
-        // one k row per lane: two converter warps per SM sub-partition, so one
-        // warp's shared-memory traffic overlaps the other's arithmetic.
-        // Shared-memory accesses: a quarter-warp covers 8 consecutive rows,
-        // whose swizzled 16-byte chunks fall on distinct banks.
+        // Warps cw = 0..3 split A rows 32q .. 32q+31 (one per lane), q = warp % 4
+        // the TMEM lane quarter the warp may write; warps 4..7 split the 32 k
+        // rows of B box cw - 4 (columns 32(cw-4) .. +31), one k row per lane:
+        // two converter warps per SM sub-partition, so one warp's memory
+        // traffic overlaps the other's arithmetic. Shared-memory accesses: a
+        // quarter-warp covers 8 consecutive rows, whose swizzled 16-byte chunks
+        // fall on distinct banks.
         const int cwx = warp - CONV0;
         const bool conv_a = cwx < Cf::NCONV / 2;
         const int cw = conv_a ? cwx : cwx - Cf::NCONV / 2;
@@ -1234,24 +1265,33 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
                 uint8_t* oa = ops + (size_t)ostage * Cf::OP_STAGE;
                 if (conv_a) {
                     // A row r: 32 FP32 k's (128-byte row, 128-byte swizzle) ->
-                    // three 64-byte BF16 rows (64-byte swizzle).
-                    const int r = cw * 32 + lane;
+                    // three limbs of 16 packed k pairs, stored in TMEM lane r at
+                    // columns A_COL + A_SLOT ostage + 16 p + pair.
+                    const int quarter = warp & 3;
+                    const int r = quarter * 32 + lane;
                     float x[32];
 #pragma unroll
                     for (int c = 0; c < 8; c++) {
                         const float4 v = *reinterpret_cast<const float4*>(sa + r * 128 + ((c ^ (r & 7)) << 4));
                         x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
                     }
+                    // The MMAs that read this slot (two stages back) are done.
+                    tc_fence_after();
+                    const uint32_t ta = tmem_base + ((uint32_t)(quarter * 32) << 16) + Cf::A_COL +
+                                        (uint32_t)ostage * Cf::A_SLOT;
 #pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        uint32_t l0[4], l1[4], l2[4];
+                    for (int h = 0; h < 2; h++) {
+                        uint32_t l0[8], l1[8], l2[8];
 #pragma unroll
-                        for (int e = 0; e < 4; e++) bf16_limbs2(x[8 * j + 2 * e], x[8 * j + 2 * e + 1], l0[e], l1[e], l2[e]);
-                        const int off = r * 64 + ((j ^ ((r >> 1) & 3)) << 4);
-                        *reinterpret_cast<uint4*>(oa + off) = make_uint4(l0[0], l0[1], l0[2], l0[3]);
-                        *reinterpret_cast<uint4*>(oa + Cf::A_PLANE + off) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
-                        *reinterpret_cast<uint4*>(oa + 2 * Cf::A_PLANE + off) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
+                        for (int e = 0; e < 8; e++)
+                            bf16_limbs2(x[16 * h + 2 * e], x[16 * h + 2 * e + 1], l0[e], l1[e], l2[e]);
+                        tmem_st_32x32b_x8(ta + (uint32_t)(8 * h), l0);
+                        tmem_st_32x32b_x8(ta + (uint32_t)(16 + 8 * h), l1);
+                        tmem_st_32x32b_x8(ta + (uint32_t)(32 + 8 * h), l2);
                     }
+                    // The limbs are in TMEM before the MMA warp is told.
+                    tmem_wait_st();
+                    tc_fence_before();
                 } else {
                     // B row k of box cw: 32 FP32 n's -> four 16-byte chunks of
                     // 8 BF16 in column panel cw / 2, chunks 4 (cw % 2) .. +3.
@@ -1263,7 +1303,7 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
                         const float4 v = *reinterpret_cast<const float4*>(sb + k * 128 + ((c ^ (k & 7)) << 4));
                         x[4 * c] = v.x; x[4 * c + 1] = v.y; x[4 * c + 2] = v.z; x[4 * c + 3] = v.w;
                     }
-                    uint8_t* ob = oa + Cf::P * Cf::A_PLANE + (cw >> 1) * (Cf::BK * 128) + k * 128;
+                    uint8_t* ob = oa + (cw >> 1) * (Cf::BK * 128) + k * 128;
 #pragma unroll
                     for (int j = 0; j < 4; j++) {
                         uint32_t l0[4], l1[4], l2[4];
@@ -1274,9 +1314,9 @@ __device__ __forceinline__ void fused_roles(const Src& src, const void* tmA1, co
                         *reinterpret_cast<uint4*>(ob + Cf::B_PLANE + off) = make_uint4(l1[0], l1[1], l1[2], l1[3]);
                         *reinterpret_cast<uint4*>(ob + 2 * Cf::B_PLANE + off) = make_uint4(l2[0], l2[1], l2[2], l2[3]);
                     }
+                    // The planes are read by the tensor cores (async proxy).
+                    fence_proxy_async();
                 }
-                // The planes are read by the tensor cores (async proxy).
-                fence_proxy_async();
                 __syncwarp();
                 if (lane == 0) {
                     mbar_arrive(&op_full[ostage]);
@@ -1326,9 +1366,11 @@ tc_splitk_reduce_kernel(const TcParams p) {
         const int q = (int)(i % BN);
         const int lrow = (int)((i / BN) % 128);
         const int64_t th = i / (int64_t)TILE;                   // tile * halves + half
+        const int64_t t = halves == 2 ? th >> 1 : th;
         int tm, tn;
-        tile_coords(p, th / halves, tm, tn);
-        const int64_t row = (int64_t)tm * p.bm + (th % halves) * 128 + lrow;
+        if (p.tiles <= (int64_t)UINT32_MAX) tile_coords_t<uint32_t>(p, (uint32_t)t, tm, tn);
+        else tile_coords_t<uint64_t>(p, (uint64_t)t, tm, tn);
+        const int64_t row = (int64_t)tm * p.bm + (th - t * halves) * 128 + lrow;
         const int64_t col = (int64_t)tn * BN + q;
         if (row >= p.M || col >= p.N) continue;
         const float* src = p.partial + (size_t)th * p.max_splits * TILE + (size_t)lrow * BN + (size_t)q;

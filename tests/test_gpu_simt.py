@@ -227,16 +227,19 @@ def test_host_entry_pipelined_path_matches_device_path(cuda, oracle_mod, prec):
 def test_row_shards_reassemble_the_product(cuda, oracle_mod, world):
     # Each rank's M-row shard (shard.sgemm_rows_dev), run here one after the
     # other on one device, writes exactly its rows; together they equal the
-    # whole-matrix launch bit for bit (FP32: the same chain per output).
+    # whole-matrix launch of the same plan bit for bit (FP32: the same chain
+    # per output). The plan is the picker's for the whole product, which the
+    # shards run; the whole launch is given it too, since a device-pointer
+    # v3 call may replace a doubtful pick by an exhaustive search's.
     from maxmulsk_b200 import shard
     torch = cuda
     M, K, N = 1000, 384, 200
     A, B = _inputs(oracle_mod, M, K, N, seed=31)
     dA, dB = to_dev(torch, A), to_dev(torch, B)
     dC = torch.full((M * N,), SENTINEL, device="cuda")
-    whole = torch.empty(M * N, device="cuda")
+    plan = mm.choose(M, K, N, mm.Precision.FP32)
     for r in range(world):
         assert shard.sgemm_rows_dev(dA, dB, dC, M, K, N, r, world) == 0
-    assert mm.sgemm_v3_dev(dA, dB, whole, M, K, N) == 0
-    assert mm.stream_status() == 0
-    assert bool(torch.equal(dC, whole))
+    st, whole, _ = run_plan(torch, A, B, M, K, N, plan, dA=dA, dB=dB)
+    assert st == 0 and mm.stream_status() == 0
+    assert np.array_equal(bits(dC.cpu().numpy()), bits(whole.ravel()))
