@@ -688,11 +688,12 @@ def main() -> None:
         tf32_peak = peaks["bf16_tflops"] / 2.0         # TF32 dense = half the BF16 rate
         mode_peak = (tf32_peak if prec == 1 else peaks["bf16_tflops"]) / PRODUCTS[prec]
         achieved = flops / t_gemm / 1e12
-        traffic = traffic_from_profiles(f"tc_gemm_{args.precision}_{S}.txt")
+        pair = plan.tile_m == 256
+        traffic = traffic_from_profiles(f"tc_gemm_{'pair_' if pair else ''}{args.precision}_{S}.txt")
         out["roofline"] = {
             "bound": "tensor", "achieved": achieved, "peak": mode_peak, "unit": "TFLOP/s",
             "frac": achieved / mode_peak, "traffic": traffic,
-            "kernel": "tc_gemm_kernel (GEMM alone, planes already split)",
+            "kernel": f"{'tc_gemm_pair_kernel' if pair else 'tc_gemm_kernel'} (GEMM alone, planes already split)",
             "peak_basis": f"{peak_src} bf16 burst {peaks['bf16_tflops']} TF/s"
                           f"{' / 2 (TF32 rate)' if prec == 1 else ''} / {PRODUCTS[prec]} products; useful 2MNK flops",
             "gemm_ms": t_gemm * 1e3, "prepass_ms": max(0.0, (t_step - t_gemm) * 1e3),
