@@ -142,11 +142,18 @@ bool parse_config_env(maxmulsk_plan& out) {
 }
 
 // Tuning database entry for this exact shape, else the learned cost model,
-// else the rule.
+// else the rule. BF16X9 has no candidates or model class of its own: it
+// takes the model's BF16X6 plan for the shape (the same tiles, K splits and
+// variants run the nine products per k instead of six; the accuracy bar is
+// asserted for every such plan).
 maxmulsk_plan choose_tuned(size_t M, size_t K, size_t N, int precision, int sms) {
     maxmulsk_plan p;
     if (tuning_lookup(M, K, N, precision, &p)) return p;
-    if (tuning_predict(M, K, N, precision, &p)) return p;
+    const int model_precision = precision == MAXMULSK_PREC_BF16X9 ? MAXMULSK_PREC_BF16X6 : precision;
+    if (tuning_predict(M, K, N, model_precision, &p)) {
+        if (precision == MAXMULSK_PREC_BF16X9) p.precision = MAXMULSK_PREC_BF16X9;
+        return p;
+    }
     return choose_rule(M, K, N, precision, sms);
 }
 

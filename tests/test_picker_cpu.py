@@ -161,6 +161,23 @@ def test_picker_doubt_triggers(built_lib, monkeypatch):
     assert mm.picker_doubt(100, 20000, 30) is None
 
 
+def test_choose_precisions_with_the_model(built_lib, monkeypatch):
+    # The model's plan for each class: SPLIT_AUTO comes back as a concrete
+    # split mode; BF16X9, which has no class of its own, runs the BF16X6
+    # plan of the shape (same tiles, K split and variant) with nine products.
+    monkeypatch.delenv("MAXMULSK_CONFIG", raising=False)
+    _load_shipped_model()
+    mm.lib().maxmulsk_tuning_clear()
+    for shape in [(128, 32768, 512), (300, 700, 260), (4096, 4096, 4096), (7, 9000, 33)]:
+        auto = mm.choose(*shape, mm.Precision.SPLIT_AUTO)
+        assert auto.precision in (mm.Precision.TF32X3, mm.Precision.BF16X6), (shape, auto)
+        x6 = mm.choose(*shape, mm.Precision.BF16X6)
+        x9 = mm.choose(*shape, mm.Precision.BF16X9)
+        assert x6.precision == mm.Precision.BF16X6 and x9.precision == mm.Precision.BF16X9
+        assert x9.as_tuple()[1:] == x6.as_tuple()[1:], (shape, x6, x9)
+        assert mm.classify(*shape, x9) == 0
+
+
 def test_picker_doubt_without_a_model(built_lib, monkeypatch):
     monkeypatch.delenv("MAXMULSK_AUTOTUNE", raising=False)
     mm.lib().maxmulsk_model_load(None)
