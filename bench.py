@@ -70,13 +70,27 @@ def traffic_from_profiles(name: str) -> float | None:
     return None
 
 
-def launches_per_step(plan, K: int) -> int:
+def resolved_split(plan, M: int, N: int) -> int:
+    """The K split a plan runs: its split_k, or for split_k 0 (tensor-core
+    plans) as many slices per tile as the device has work slots per tile
+    (SMs, or CTA pairs for 256-row tiles), 1..64."""
+    if plan.split_k:
+        return plan.split_k
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    slots = sms // 2 if plan.tile_m == 256 else sms
+    tiles = -(-M // plan.tile_m) * -(-N // plan.tile_n)
+    return max(1, min(64, slots // tiles))
+
+
+def launches_per_step(plan, M: int, K: int, N: int) -> int:
     """Kernels of this library one call of `plan` launches: the split pre-pass
-    (one per operand) and the tensor-core GEMM, or the SIMT GEMM; plus the
-    split-K reduction when every tile is cut into 3 or more K slices."""
+    (one per operand) and the tensor-core GEMM, the fused-split GEMM, or the
+    SIMT GEMM; plus the split-K reduction when every tile is cut into 3 or
+    more K slices."""
     import maxmulsk_b200 as mm
-    n = 1 if plan.precision == 0 else 3
-    if mm.slice_count(K, plan.split_k) >= 3:
+    n = 1 if plan.precision == 0 or plan.variant == mm.TC_FUSED_SPLIT else 3
+    if mm.slice_count(K, resolved_split(plan, M, N)) >= 3:
         n += 1
     return n
 
@@ -675,7 +689,7 @@ def main() -> None:
                    "l2": f"A+B+C = {4 * (M * K + K * N + M * N) / 2**20:.0f} MiB, workspace "
                          f"{ws_bytes / 2**20:.0f} MiB (L2 126 MB)", "parallelism": f"replicas x{world} (M-row shards)"},
         "clocks": clocks,
-        "gpu_launches": launches_per_step(plan, K) * args.steps,
+        "gpu_launches": launches_per_step(plan, M, K, N) * args.steps,
     }
 
     if not args.no_extras:

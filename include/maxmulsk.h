@@ -113,7 +113,10 @@ enum {
  *                    256 x {128, 256} on a pair of CTAs (tcgen05 cta_group::2).
  *   split_k   : number of K slices (1..64). Slices are summed in slice order,
  *               first slice first, like the reference's outer-Kc panels
- *               (sme/v3/sme-1x4-acc-kcout.cpp:464-471, 530-558).
+ *               (sme/v3/sme-1x4-acc-kcout.cpp:464-471, 530-558). Tensor-core
+ *               plans also take 0: as many slices per tile as the device has
+ *               work slots (SMs, or CTA pairs) per tile, at most 64, so one
+ *               launch runs about one equal K slice per SM.
  *   variant   : FP32: MAXMULSK_FP32_FMA or MAXMULSK_FP32_SCALAR.
  *               Tensor cores: MAXMULSK_TC_SPLIT_INPUTS, MAXMULSK_TC_REUSE_PLANES or
  *               MAXMULSK_TC_FUSED_SPLIT.

@@ -36,14 +36,15 @@ int candidate_plans(int cls, maxmulsk_plan* out, int cap) {
             for (int sk : splits) add(MAXMULSK_PREC_FP32, t[0], t[1], sk);
     } else {
         // 18 + 18 planes-in-memory plans, 7 fused-split plans (narrow shapes
-        // need deep K splits), 5 narrow-tile plans: 48.
+        // need deep K splits; split 0 fills the SMs with one K slice per
+        // slot), 5 narrow-tile plans: 48.
         const int modes[2] = {MAXMULSK_PREC_3XTF32, MAXMULSK_PREC_BF16X6};
         const int tiles[3][2] = {{128, 128}, {128, 256}, {256, 256}};
         const int splits[6] = {1, 2, 4, 8, 16, 32};
         for (int m : modes)
             for (auto& t : tiles)
                 for (int sk : splits) add(m, t[0], t[1], sk);
-        const int fused_splits[7] = {1, 2, 4, 8, 16, 32, 64};
+        const int fused_splits[7] = {1, 2, 4, 8, 16, 32, 0};
         for (int sk : fused_splits) add(MAXMULSK_PREC_BF16X6, 128, 128, sk, MAXMULSK_TC_FUSED_SPLIT);
         add(MAXMULSK_PREC_3XTF32, 128, 64, 4);
         add(MAXMULSK_PREC_3XTF32, 128, 64, 16);

@@ -33,7 +33,10 @@ constexpr size_t kMaxDim = 0x7FFFFFFFull;   // TMA coordinates and grid sizes ar
 maxmulsk_status classify_plan(size_t M, size_t K, size_t N, const maxmulsk_plan* plan) {
     if (!plan) { set_error_message("null plan"); return MAXMULSK_ERR_INVALID; }
     const maxmulsk_plan& p = *plan;
-    if (p.split_k < 1 || p.split_k > 64) { set_error_message("split_k must be 1..64"); return MAXMULSK_ERR_UNSUPPORTED; }
+    if (p.split_k < 0 || p.split_k > 64 || (p.split_k == 0 && p.precision == MAXMULSK_PREC_FP32)) {
+        set_error_message("split_k must be 1..64 (0: fill the SMs, tensor-core plans only)");
+        return MAXMULSK_ERR_UNSUPPORTED;
+    }
     if (p.precision == MAXMULSK_PREC_FP32) {
         const bool tile_ok = (p.tile_m == 128 && p.tile_n == 128) || (p.tile_m == 128 && p.tile_n == 64) ||
                              (p.tile_m == 64 && p.tile_n == 64);

@@ -1415,12 +1415,19 @@ Sched make_sched(int64_t M, int64_t K, int64_t N, int tile_m, int tile_n, int sp
     s.tiles_m = (M + tile_m - 1) / tile_m;
     s.tiles_n = (N + tile_n - 1) / tile_n;
     s.tiles = s.tiles_m * s.tiles_n;
+    if (sms <= 0) sms = 148;                        // work slots: SMs, or resident CTA pairs
+    if (split_k == 0) {
+        // Fill the machine: every tile cut into as many K slices as there are
+        // slots per tile, so the units number about one per slot and each runs
+        // the same number of k-steps (a stream-K schedule in whole slices).
+        const int64_t f = sms / s.tiles;
+        split_k = (int)(f < 1 ? 1 : (f > 64 ? 64 : f));
+    }
     s.main_splits = slice_count((size_t)K, split_k);
     s.main_kchunk = (int64_t)slice_len((size_t)K, split_k);
     s.main_tiles = s.tiles;
     s.tail_splits = 1;
     s.tail_kchunk = K;
-    if (sms <= 0) sms = 148;                        // work slots: SMs, or resident CTA pairs
     if (s.main_splits == 1 && s.tiles > sms) {
         const int64_t r = s.tiles % sms;
         if (r > 0 && r <= sms / 2) {
