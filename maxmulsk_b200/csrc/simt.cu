@@ -502,7 +502,7 @@ simt_splitk_reduce_kernel(const float* __restrict__ partial, float* __restrict__
     const size_t MN = (size_t)M * (size_t)N;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)MN;
          i += (int64_t)gridDim.x * blockDim.x)
-        C[i] = ordered_sum(partial + i, MN, splits);
+        C[i] = ordered_sum<64>(partial + i, MN, splits);
 }
 
 // Slices at or above which the partials are summed by the reduction kernel.

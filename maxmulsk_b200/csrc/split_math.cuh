@@ -38,15 +38,17 @@ __device__ __forceinline__ void bf16_limbs2(float x0, float x1, uint32_t& p0, ui
 
 // src[0] + src[stride] + ... + src[(n - 1) stride], added in that order with
 // round-to-nearest FP32 adds (the slice order of the split-K reductions); the
-// loads are issued 16 at a time so that they overlap.
+// loads are issued BATCH at a time so that they overlap (a batch of 64 covers
+// every split in one round trip to L2).
+template <int BATCH = 16>
 __device__ __forceinline__ float ordered_sum(const float* __restrict__ src, size_t stride, int n) {
     float acc = __ldcs(src);
-    for (int z = 1; z < n; z += 16) {
-        float v[16];
+    for (int z = 1; z < n; z += BATCH) {
+        float v[BATCH];
 #pragma unroll
-        for (int j = 0; j < 16; j++) v[j] = (z + j < n) ? __ldcs(src + (size_t)(z + j) * stride) : 0.0f;
+        for (int j = 0; j < BATCH; j++) v[j] = (z + j < n) ? __ldcs(src + (size_t)(z + j) * stride) : 0.0f;
 #pragma unroll
-        for (int j = 0; j < 16; j++)
+        for (int j = 0; j < BATCH; j++)
             if (z + j < n) acc = __fadd_rn(acc, v[j]);
     }
     return acc;

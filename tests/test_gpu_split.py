@@ -83,7 +83,7 @@ TC_TILES = [(128, 64), (128, 128), (128, 256), (256, 128), (256, 256)]
 
 @pytest.mark.parametrize("prec", MODES)
 @pytest.mark.parametrize("tile", TC_TILES)
-@pytest.mark.parametrize("split_k", [1, 3])
+@pytest.mark.parametrize("split_k", [1, 3, 0])
 def test_tc_gemm_vs_exact_split_product(cuda, oracle_mod, prec, tile, split_k):
     for i, (M, K, N) in enumerate(SHAPES):
         A = oracle_mod.fill_uniform(M * K, 30 + i)
@@ -192,11 +192,12 @@ FUSED_SHAPES = [(128, 128, 128), (68, 68, 68), (20, 36, 40), (300, 520, 200), (2
 
 
 @pytest.mark.parametrize("prec", [mm.Precision.BF16X6, mm.Precision.BF16X9])
-@pytest.mark.parametrize("split_k", [1, 2, 5])
+@pytest.mark.parametrize("split_k", [1, 2, 5, 0])
 def test_fused_split_equals_split_inputs(cuda, oracle_mod, prec, split_k):
-    # The fused kernel splits FP32 tiles into limb planes in shared memory;
-    # the products, their order and the chunked accumulation are those of the
-    # split-inputs path on the same tiles, so C must agree bit for bit.
+    # The fused kernel splits FP32 tiles into limbs itself (A's into tensor
+    # memory, B's into shared memory); the products, their order and the
+    # chunked accumulation are those of the split-inputs path on the same
+    # tiles, so C must agree bit for bit.
     for i, (M, K, N) in enumerate(FUSED_SHAPES):
         A = np.concatenate([oracle_mod.fill_uniform(M * K // 2, 200 + i),
                             oracle_mod.fill_wide(M * K - M * K // 2, 300 + i)])
@@ -221,3 +222,25 @@ def test_fused_split_unaligned_inputs_take_the_split_inputs_path(cuda, oracle_mo
     assert st == 0 and bands
     _, Cref, _ = run_plan(cuda, A, B, M, K, N, mm.make_plan(mm.Precision.BF16X6, 128, 128, 1))
     assert np.array_equal(bits(C), bits(Cref))
+
+
+@pytest.mark.parametrize("variant", [mm.TC_SPLIT_INPUTS, mm.TC_FUSED_SPLIT])
+@pytest.mark.parametrize("shape", [(128, 32768, 512), (64, 8192, 512), (300, 2048, 700)])
+def test_fill_split_is_the_slots_per_tile_split(cuda, oracle_mod, variant, shape):
+    # split_k 0 cuts every tile into as many K slices as the device has SMs
+    # per tile (at most 64): the same schedule, and so the same bits, as the
+    # plan that names that split.
+    torch = cuda
+    M, K, N = shape
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    tiles = -(-M // 128) * -(-N // 128)
+    want = max(1, min(64, sms // tiles))
+    A = oracle_mod.fill_uniform(M * K, 501)
+    B = oracle_mod.fill_uniform(K * N, 502)
+    dA, dB = to_dev(torch, A), to_dev(torch, B)
+    prec = mm.Precision.BF16X6
+    st0, C0, b0 = run_plan(torch, A, B, M, K, N, mm.make_plan(prec, 128, 128, 0, variant), dA=dA, dB=dB)
+    st1, C1, b1 = run_plan(torch, A, B, M, K, N, mm.make_plan(prec, 128, 128, want, variant), dA=dA, dB=dB)
+    assert st0 == 0 and st1 == 0, mm.last_error_message()
+    assert b0 and b1
+    assert np.array_equal(bits(C0), bits(C1)), (shape, want)
