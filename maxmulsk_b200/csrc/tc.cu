@@ -144,7 +144,7 @@ struct TcParams {
     int reduce_after;        // split tiles only write partials; tc_splitk_reduce_kernel sums them
     int store_c;             // whole tiles leave through the C tensor map (TMA stores)
     float* C;
-    float* partial;          // [split tile][slice][128 x BN], split tiles only
+    float* partial;          // [split tile][slice][BN columns x 128 rows], column-major, split tiles only
     unsigned* counters;      // EPI per split tile (one per epilogue warp)
     int* err;
     long long timeout;       // SM clocks per bounded wait
@@ -211,7 +211,7 @@ struct UnitView {
     int problem;             // index in a grouped launch (0 for one GEMM)
     int64_t M, N;
     float* C;
-    float* partial;          // the problem's partial tiles: [split tile][slice][128 x BN]
+    float* partial;          // the problem's partial tiles: [split tile][slice][BN x 128], column-major
     unsigned* counters;      // the problem's arrival counters: EPI per split tile
     int max_splits;          // slices per split tile in the partial layout
     int chunk_kb;            // stages per TMEM accumulation chunk
@@ -290,20 +290,21 @@ __device__ __forceinline__ void store_row_regs(const float (&sum)[COLS], float* 
 }
 
 // A K slice z of a split tile: this thread's row segment goes into the
-// slice's partial tile (`seg` = the segment in slice 0; slices `tile` floats
-// apart, compact whole rows). Unless a reduction kernel sums the slices
-// (`reduce_after`), the last slice to arrive on this warp's counter reads
-// every slice back in slice order (its own included, 128-bit loads), sums
-// them with round-to-nearest adds, stores the segment of C and resets the
-// counter.
+// slice's partial tile (`seg` = the segment's first element in slice 0;
+// slices `tile` floats apart). Partial tiles are column-major, 128 rows per
+// column (element (r, c) at c * 128 + r), so the 32 lanes of a warp, 32
+// consecutive rows, store each column as one contiguous 128-byte line.
+// Unless a reduction kernel sums the slices (`reduce_after`), the last slice
+// to arrive on this warp's counter reads every slice back in slice order (its
+// own included), sums them with round-to-nearest adds, stores the segment of
+// C and resets the counter.
 template <int COLS>
 __device__ __forceinline__ void finish_slice(float (&sum)[COLS], float* seg, size_t tile, int z, int nsplit,
                                              bool reduce_after, unsigned* ctr, int lane, float* C, int64_t row,
                                              int64_t col0, int64_t M, int64_t N, bool vec) {
     float* part = seg + (size_t)z * tile;
 #pragma unroll
-    for (int j = 0; j < COLS; j += 4)
-        __stcg(reinterpret_cast<float4*>(part + j), make_float4(sum[j], sum[j + 1], sum[j + 2], sum[j + 3]));
+    for (int j = 0; j < COLS; j++) __stcg(part + (size_t)j * 128, sum[j]);
     if (reduce_after) return;
     __threadfence();
     __syncwarp();
@@ -313,20 +314,11 @@ __device__ __forceinline__ void finish_slice(float (&sum)[COLS], float* seg, siz
     if (!last) return;
     __threadfence();
 #pragma unroll
-    for (int j = 0; j < COLS; j += 4) {
-        const float4 t = __ldcg(reinterpret_cast<const float4*>(seg + j));
-        sum[j] = t.x; sum[j + 1] = t.y; sum[j + 2] = t.z; sum[j + 3] = t.w;
-    }
+    for (int j = 0; j < COLS; j++) sum[j] = __ldcg(seg + (size_t)j * 128);
     for (int q = 1; q < nsplit; q++) {
         const float* bq = seg + (size_t)q * tile;
 #pragma unroll
-        for (int j = 0; j < COLS; j += 4) {
-            const float4 t = __ldcg(reinterpret_cast<const float4*>(bq + j));
-            sum[j] = __fadd_rn(sum[j], t.x);
-            sum[j + 1] = __fadd_rn(sum[j + 1], t.y);
-            sum[j + 2] = __fadd_rn(sum[j + 2], t.z);
-            sum[j + 3] = __fadd_rn(sum[j + 3], t.w);
-        }
+        for (int j = 0; j < COLS; j++) sum[j] = __fadd_rn(sum[j], __ldcg(bq + (size_t)j * 128));
     }
     store_row_regs<COLS>(sum, C, row, col0, M, N, vec);
     if (lane == 0) *ctr = 0u;
@@ -410,7 +402,7 @@ __device__ __forceinline__ void epilogue_role(const Src& src, int* err, long lon
             continue;
         }
         constexpr size_t TILE = (size_t)Cf::BM * BN;
-        finish_slice<COLS>(sum, v.partial + (size_t)w.sti * v.max_splits * TILE + (size_t)lrow * BN + lcol, TILE, w.z,
+        finish_slice<COLS>(sum, v.partial + (size_t)w.sti * v.max_splits * TILE + (size_t)lcol * 128 + lrow, TILE, w.z,
                            w.nsplit, v.reduce_after != 0, v.counters + (size_t)w.sti * Cf::EPI + ew, lane, v.C, row,
                            col0, M, N, vec);
     }
@@ -799,7 +791,7 @@ tc_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_consta
             // K-split tile: this CTA's 128-row half is its own partial tile.
             constexpr size_t TILE = (size_t)Cf::HM * BN;
             const int64_t half = w.sti * 2 + rank;
-            finish_slice<COLS>(sum, p.partial + (size_t)half * p.max_splits * TILE + (size_t)lrow * BN + lcol, TILE,
+            finish_slice<COLS>(sum, p.partial + (size_t)half * p.max_splits * TILE + (size_t)lcol * 128 + lrow, TILE,
                                w.z, w.nsplit, p.reduce_after != 0, p.counters + (size_t)half * Cf::EPI + ew, lane, p.C,
                                row, col0, M, N, vec);
         }
@@ -1031,8 +1023,11 @@ __device__ __forceinline__ void epilogue_role_tsum(const Src& src, int* err, lon
             }
             continue;
         }
+        // Partial tiles column-major (element (r, c) at c * 128 + r): the 32
+        // lanes of a warp hold 32 consecutive rows, so each store of one
+        // column is one contiguous 128-byte line.
         constexpr size_t TILE = (size_t)Cf::BM * BN;
-        float* seg = v.partial + (size_t)w.sti * v.max_splits * TILE + (size_t)lrow * BN;
+        float* seg = v.partial + (size_t)w.sti * v.max_splits * TILE + (size_t)lrow;
         float* part = seg + (size_t)w.z * TILE;
 #pragma unroll
         for (int c = 0; c < BN; c += W) {
@@ -1040,10 +1035,7 @@ __device__ __forceinline__ void epilogue_role_tsum(const Src& src, int* err, lon
             tmem_ld_32x32b_x32(tsum + (uint32_t)c, q);
             tmem_wait_ld();
 #pragma unroll
-            for (int j = 0; j < W; j += 4)
-                __stcg(reinterpret_cast<float4*>(part + c + j),
-                       make_float4(__uint_as_float(q[j]), __uint_as_float(q[j + 1]), __uint_as_float(q[j + 2]),
-                                   __uint_as_float(q[j + 3])));
+            for (int j = 0; j < W; j++) __stcg(part + (size_t)(c + j) * Cf::BM, __uint_as_float(q[j]));
         }
         if (v.reduce_after) continue;
         unsigned* ctr = v.counters + (size_t)w.sti * Cf::EPI + ew;
@@ -1058,20 +1050,11 @@ __device__ __forceinline__ void epilogue_role_tsum(const Src& src, int* err, lon
         for (int c = 0; c < BN; c += W) {
             float sum[W];
 #pragma unroll
-            for (int j = 0; j < W; j += 4) {
-                const float4 t = __ldcg(reinterpret_cast<const float4*>(seg + c + j));
-                sum[j] = t.x; sum[j + 1] = t.y; sum[j + 2] = t.z; sum[j + 3] = t.w;
-            }
+            for (int j = 0; j < W; j++) sum[j] = __ldcg(seg + (size_t)(c + j) * Cf::BM);
             for (int qz = 1; qz < w.nsplit; qz++) {
-                const float* bq = seg + (size_t)qz * TILE + c;
+                const float* bq = seg + (size_t)qz * TILE;
 #pragma unroll
-                for (int j = 0; j < W; j += 4) {
-                    const float4 t = __ldcg(reinterpret_cast<const float4*>(bq + j));
-                    sum[j] = __fadd_rn(sum[j], t.x);
-                    sum[j + 1] = __fadd_rn(sum[j + 1], t.y);
-                    sum[j + 2] = __fadd_rn(sum[j + 2], t.z);
-                    sum[j + 3] = __fadd_rn(sum[j + 3], t.w);
-                }
+                for (int j = 0; j < W; j++) sum[j] = __fadd_rn(sum[j], __ldcg(bq + (size_t)(c + j) * Cf::BM));
             }
             store_row_regs<W>(sum, v.C, row, col0 + c, M, N, vec);
         }
@@ -1363,8 +1346,10 @@ tc_splitk_reduce_kernel(const TcParams p) {
     const int64_t total = p.tiles * halves * (int64_t)TILE;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const int q = (int)(i % BN);
-        const int lrow = (int)((i / BN) % 128);
+        // Partial tiles are column-major (c * 128 + r): consecutive threads
+        // read consecutive partial elements down a column.
+        const int lrow = (int)(i % 128);
+        const int q = (int)((i / 128) % BN);
         const int64_t th = i / (int64_t)TILE;                   // tile * halves + half
         const int64_t t = halves == 2 ? th >> 1 : th;
         int tm, tn;
@@ -1373,7 +1358,7 @@ tc_splitk_reduce_kernel(const TcParams p) {
         const int64_t row = (int64_t)tm * p.bm + (th - t * halves) * 128 + lrow;
         const int64_t col = (int64_t)tn * BN + q;
         if (row >= p.M || col >= p.N) continue;
-        const float* src = p.partial + (size_t)th * p.max_splits * TILE + (size_t)lrow * BN + (size_t)q;
+        const float* src = p.partial + (size_t)th * p.max_splits * TILE + (size_t)q * 128 + (size_t)lrow;
         p.C[(size_t)row * (size_t)p.N + (size_t)col] = ordered_sum(src, TILE, p.main_splits);
     }
 }
