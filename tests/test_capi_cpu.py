@@ -52,6 +52,9 @@ def test_status_codes_keep_reference_values(built_lib):
     ((3, 128, 128, 1, 0), True), ((1, 64, 128, 1, 0), False), ((1, 128, 96, 1, 0), False),
     ((1, 256, 256, 1, 0), True), ((2, 256, 128, 3, 0), True), ((1, 256, 64, 1, 0), False),
     ((1, 128, 128, 1, 1), True), ((1, 128, 128, 1, 2), False), ((4, 128, 128, 1, 0), False), ((-1, 128, 128, 1, 0), False),
+    # split_k 0: one K slice per SM for every tile, tensor-core plans only
+    ((1, 128, 256, 0, 0), True), ((2, 256, 256, 0, 0), True), ((2, 128, 128, 0, 2), True), ((3, 128, 128, 0, 2), True),
+    ((2, 128, 128, -1, 0), False),
 ])
 def test_classify(built_lib, plan, ok):
     p = mm.make_plan(*plan)
